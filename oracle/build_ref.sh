@@ -1,0 +1,25 @@
+#!/usr/bin/env bash
+# Compiles the reference's own exact CPU counters, straight from the reference
+# sources, into oracle/_ref/ (git-ignored). These are the pins for the C
+# restatement in hm_oracle.c and the timed CPU baseline. Nothing is copied:
+# g++ reads the sources where they lie.
+#   MoCHy-master/main_exact.cpp       -> _ref/mochy_exact
+#   MoCHy-master/main_exact_par.cpp   -> _ref/mochy_exact_par   (OpenMP)
+#   THyMe-main/code/main_thyme.cpp    -> _ref/thyme
+#   THyMe-main/code/main_thymeP.cpp   -> _ref/thymeP            (OpenMP)
+set -euo pipefail
+REF=${HM_REFERENCE_ROOT:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+if [ ! -d "$REF/MoCHy-master" ] || [ ! -d "$REF/THyMe-main/code" ]; then
+  echo "build_ref.sh: reference tree not found at $REF; keeping existing _ref/" >&2
+  exit 0
+fi
+mkdir -p "$OUT"
+# The system g++ carries libgomp; a bare $CXX from the environment may not.
+CXX=${HM_REF_CXX:-$( [ -x /usr/bin/g++ ] && echo /usr/bin/g++ || echo g++ )}
+$CXX -O3 -std=c++11 -o "$OUT/mochy_exact" "$REF/MoCHy-master/main_exact.cpp"
+$CXX -O3 -std=c++11 -fopenmp -o "$OUT/mochy_exact_par" "$REF/MoCHy-master/main_exact_par.cpp"
+$CXX -O3 -std=c++11 -o "$OUT/thyme" "$REF/THyMe-main/code/main_thyme.cpp"
+$CXX -O3 -std=c++11 -fopenmp -o "$OUT/thymeP" "$REF/THyMe-main/code/main_thymeP.cpp"
+echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"
