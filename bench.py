@@ -1,0 +1,326 @@
+"""Benchmark: hyperedge triples classified per second on the 2M-hyperedge
+static workload (config 2), plus the update-batch latency of the dynamic
+workload when that path is enabled.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...
+
+A step is one exact static count (all 30 classes, i.e. MoCHy's 26 motifs plus
+the four repeated-hyperedge classes) of the resident graph. With N GPUs every
+rank holds a replica of the graph and counts one shard of the centres; the
+30-class partial counts are summed with one NCCL all-reduce per step, so the
+total work is fixed (strong scaling). Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "hyperedge triples classified/sec at 2M edges; update-batch p50/p99 latency"
+UNIT = "triples/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--edges", type=int, default=2_000_000)
+    ap.add_argument("--nodes", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-traffic", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def workload(args):
+    from ipdps26_b200 import gen
+
+    q = gen.C2_Q * args.edges / 2_000_000
+    p = gen.config2(seed=1, n_nodes=args.nodes, n_edges=args.edges, q=q)
+    return p, gen.static(p)
+
+
+def config_of(args, n_gpus):
+    from ipdps26_b200 import gen
+
+    return {
+        "workload": "config2-static-count",
+        "hyperedges": args.edges,
+        "nodes": args.nodes,
+        "sizes": "k^-2.2 on [2,100]",
+        "popularity": f"Zipf-Mandelbrot s=1.1 q={gen.C2_Q * args.edges / 2_000_000:g}",
+        "seed": 1,
+        "parallelism": f"centre-shard x{n_gpus} (replicated store)" if n_gpus > 1 else "single GPU",
+        "l2": "inputs larger than L2 (store of tens of GB per step)",
+    }
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for ln in out.splitlines():
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(h, budget_s: float):
+    """The reference's own OpenMP counter (MoCHy main_exact_par, built from the
+    reference sources into oracle/_ref) on all host cores, on a bounded
+    sample: the first E' hyperedges of the same workload, E' doubled until
+    one run takes about budget_s."""
+    from oracle import ref_runner as rr
+
+    if not rr.available("mochy_exact_par"):
+        return None
+    cores = os.cpu_count() or 1
+    n = min(10_000, h.n_edges)
+    best = None
+    while n <= h.n_edges:
+        sub = h.subgraph(n)
+        try:
+            counts, wall, _ = rr.run_mochy(sub.offsets, sub.members, threads=cores, timeout=max(120, budget_s * 8))
+        except Exception as e:  # noqa: BLE001
+            if best is None:
+                return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                        "sample": f"failed at {n} hyperedges: {e}"}
+            break
+        best = (n, int(counts.sum()), wall)
+        if wall >= budget_s or n == h.n_edges:
+            break
+        n = min(h.n_edges, n * 2)
+    n, triples, wall = best
+    return {"value": triples / wall, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"MoCHy main_exact_par, first {n} hyperedges of the workload (same laws and node universe), "
+                      f"{triples} triples (26 motifs) in {wall:.2f} s wall including its file parse",
+            "wall_s": wall, "sample_hyperedges": n}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    p, h = workload(args)
+    base = cpu_baseline(h, args.cpu_sample_seconds)
+    cfg = config_of(args, 1)
+    if base is None or base.get("value") is None:
+        why = "reference counter (oracle/_ref) not built here" if base is None else base["sample"]
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    n = base["sample_hyperedges"]
+    sub = h.subgraph(n)
+    from oracle import ref_runner as rr
+
+    cores = base["cores"]
+    for _ in range(args.warmup):
+        rr.run_mochy(sub.offsets, sub.members, threads=cores)
+    walls, triples = [], 0
+    for _ in range(args.steps):
+        c, w, _ = rr.run_mochy(sub.offsets, sub.members, threads=cores)
+        walls.append(w)
+        triples = int(c.sum())
+    t = sum(walls)
+    value = triples * args.steps / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def engine_arm(args, rank, world, local_rank):
+    import torch
+
+    from ipdps26_b200 import engine
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    p, h = workload(args)
+    ctx = engine.Context(local_rank)
+    g = engine.Graph.from_hypergraph(ctx, h)
+    stream = torch.cuda.ExternalStream(engine.lib.hm_ctx_stream(ctx.handle))
+
+    def step():
+        part = g.count_static30_shard(rank, world)
+        if world > 1:
+            t = torch.from_numpy(part.view(np.int64)).to(f"cuda:{local_rank}")
+            dist.all_reduce(t)
+            part = t.cpu().numpy().view(np.uint64)
+        return part
+
+    for _ in range(args.warmup):
+        counts = step()
+    closed_ms, open_ms = [], []
+    with ClockSampler(local_rank) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            counts = step()
+            t = g.timings()
+            closed_ms.append(t.closed_ms)
+            open_ms.append(t.open_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if world > 1:
+            dist.barrier()
+    dev_s = e0.elapsed_time(e1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([dev_s], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_s = float(tt.item())
+    triples = int(counts.astype(np.uint64).sum())
+    value = triples * args.steps / dev_s
+
+    result = None
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        info = g.info()
+        roof = None
+        if not args.no_traffic:
+            tr = g.traffic()
+            # one step = the two count kernels; per-launch duration from events
+            t_launch = (statistics.mean(closed_ms) + statistics.mean(open_ms)) / 1000.0
+            achieved = tr.b_static / t_launch / 1e9
+            traffic = None
+            tp = ROOT / "profiles" / "static_count_traffic.json"
+            if tp.exists():
+                tj = json.loads(tp.read_text())
+                if tj.get("hyperedges") == args.edges:
+                    traffic = tj.get("dram_bytes_per_step")
+            roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "traffic": traffic, "peak_kind": peak_kind,
+                    "algorithmic_bytes": tr.b_static, "kernel_model_bytes": tr.kernel_bytes,
+                    "kernel_model_gbs": tr.kernel_bytes / t_launch / 1e9,
+                    "kernel": "k_closed + k_open_pairs (one static count)",
+                    "closed_ms": statistics.mean(closed_ms), "open_ms": statistics.mean(open_ms)}
+        e2e = None
+        if not args.no_e2e:
+            # through the public API from host buffers: build (H2D of the CSR),
+            # count, read the 26 counts back; pinned host copies of the inputs
+            off = torch.from_numpy(h.offsets.view(np.int64)).pin_memory().numpy().view(np.uint64)
+            mem = torch.from_numpy(h.members.view(np.int32)).pin_memory().numpy().view(np.uint32)
+            times = []
+            for _ in range(args.e2e_steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                with engine.Graph(ctx, off, mem, h.n_nodes) as g2:
+                    c26 = g2.count_static()
+                times.append(time.perf_counter() - t0)
+            e2e = {"value": int(c26.sum()) / statistics.mean(times), "unit": UNIT,
+                   "h2d_bytes_per_step": int(off.nbytes + mem.nbytes), "d2h_bytes_per_step": 26 * 8,
+                   "s_per_step": statistics.mean(times),
+                   "note": "26 reported motifs; build of H2V/V2H/H2H included"}
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            base = cpu_baseline(h, args.cpu_sample_seconds)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": config_of(args, world), "gpu_launches": 2 * args.steps,
+            "triples_per_step": triples, "closed_triangles_per_step": int(g.timings().closed_triangles),
+            "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
+            "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
+                      "device_gb": info.device_bytes / 1e9},
+        }
+        print(json.dumps(result), flush=True)
+    g.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if "RANK" not in os.environ:
+        world = 1 if args.gpus == 1 else args.gpus
+        if world != 1:
+            raise SystemExit("for --gpus > 1 launch with torchrun (one process per GPU)")
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        engine_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -104,6 +104,110 @@ int hm_gen_batch(const hm_gen_params* p, uint64_t batch_seed, const uint32_t* li
 int hm_hostgraph_view(const hm_hostgraph* hg, hm_hostgraph_info* info);
 void hm_hostgraph_free(hm_hostgraph* hg);
 
+/* ---- contexts --------------------------------------------------------- */
+typedef struct hm_ctx hm_ctx;
+typedef struct hm_graph hm_graph;
+
+/* A context binds one CUDA device and one stream; every device byte the
+ * engine allocates through it is charged against mem_budget_bytes (0 = the
+ * device's free memory at creation). Calls on one context are serialised.
+ * Replaces the per-store cudaMalloc bookkeeping of CBSTOperations
+ * (dynamicHyperGraph/structure/operations.cu:359-374), which exits the
+ * process on any CUDA error. */
+int hm_ctx_create(int device, size_t mem_budget_bytes, hm_ctx** out);
+int hm_ctx_destroy(hm_ctx* ctx);
+int hm_ctx_memory(const hm_ctx* ctx, size_t* used_bytes, size_t* budget_bytes);
+/* The context's cudaStream_t, as void* so this header needs no CUDA types. */
+void* hm_ctx_stream(const hm_ctx* ctx);
+/* Test hook: after n further successful device allocations, allocations fail
+ * with HM_ERR_NOMEM (n < 0 switches the hook off). */
+int hm_debug_fail_allocations_after(long long n);
+
+/* ---- the device store ------------------------------------------------- */
+/* Builds H2V (hyperedge -> sorted members), V2H (node -> sorted hyperedges)
+ * and H2H (hyperedge -> adjacent hyperedges with overlap sizes) on the
+ * device from a host CSR: hyperedge e (id e) has members
+ * members[offsets[e] .. offsets[e+1]), node ids < n_nodes. timestamps may be
+ * NULL (static graph) or hold one int64 per hyperedge (temporal graph).
+ * Replaces constructCBST (dynamicHyperGraph/structure/operations.cu:31-80)
+ * for all three stores plus the host H2H builder hyperedgeAdjacency
+ * (dynamicHyperGraph/utils/utils.cpp:399-427). */
+int hm_graph_build(hm_ctx* ctx, const uint64_t* offsets, const uint32_t* members, uint32_t n_edges,
+                   uint32_t n_nodes, const int64_t* timestamps, hm_graph** out);
+int hm_graph_destroy(hm_graph* g);
+
+typedef struct hm_graph_info_t {
+  uint32_t n_slots;     /* ids in use or free: 0 .. n_slots-1 */
+  uint32_t n_live;
+  uint32_t n_nodes;
+  int32_t temporal;
+  uint64_t n_members;   /* H2V entries */
+  uint64_t n_adjacent;  /* H2H entries (both directions) */
+  uint64_t n_oriented;  /* oriented H2H entries (0 until the first count) */
+  uint64_t device_bytes;/* bytes charged to the context */
+} hm_graph_info_t;
+int hm_graph_info(const hm_graph* g, hm_graph_info_t* info);
+
+/* Member lists of live hyperedges ids[0..n): offsets_out[0..n] (CSR) and
+ * members_out (capacity members_cap). Replaces findAndPrint / findContents
+ * (dynamicHyperGraph/structure/operations.cu:425-433, kernel/find.cu:26-51),
+ * which only print. HM_ERR_NOT_LIVE if an id is free or out of range. */
+int hm_graph_query(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t* offsets_out, uint32_t* members_out,
+                   size_t members_cap);
+
+/* ---- counts ------------------------------------------------------------ */
+/* MoCHy's 26 static h-motif counts over all connected hyperedge triples.
+ * Replaces computeMotifCounts (dynamicHyperGraph/include/motif.hpp:10-13,
+ * src/HMotifCount.cu:97-125), which returns nothing and counts closed
+ * triangles only; the numbers are those of MoCHy main_exact
+ * (MoCHy-master/main_exact.cpp:91-137). */
+int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]);
+/* The same in the reference's 30-bin order (classes 0, 1, 4, 6 are non-zero
+ * only when hyperedges repeat). */
+int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]);
+
+/* Partial 30-class counts over one shard of the centres: the sum over
+ * shard = 0 .. n_shards-1 equals hm_count_static30. One shard per GPU, each
+ * GPU holding a replica of the graph, gives the multi-GPU count with a
+ * single 30 x uint64 sum across ranks. */
+int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[HM_N_STATIC_CLASSES]);
+
+/* Algorithmic bytes of one static count of this graph (for rooflines):
+ * b_static follows the reference-equivalent merge algorithm
+ * (MoCHy-master/main_exact.cpp:91-129): store read once
+ * (4 nnz(H2V) + 8 nnz(H2H)), sum over id-ordered adjacent pairs of
+ * 8 (d+(a) + d+(b)) with d+ the neighbours of larger id, and
+ * 4 (|a| + |b|) per pair that closes a triangle. kernel_bytes is what this
+ * engine's kernels read. Runs one extra diagnostic count (slow). */
+typedef struct hm_traffic_t {
+  uint64_t store_bytes;
+  uint64_t merge_bytes;
+  uint64_t closed_pair_bytes;
+  uint64_t b_static;
+  uint64_t probes;          /* hash probes of the closed phase */
+  uint64_t kernel_bytes;
+  uint64_t closed_triangles;
+} hm_traffic_t;
+int hm_graph_traffic(hm_graph* g, hm_traffic_t* t);
+
+/* Device times of the last count / update call on this graph (CUDA events
+ * on the context stream). */
+typedef struct hm_timings_t {
+  float open_ms;     /* open-pair phase of the static count */
+  float closed_ms;   /* closed-triangle phase of the static count */
+  float count_ms;    /* whole static count */
+  float update_ms;   /* last batch update */
+  float temporal_ms; /* last temporal count */
+  uint64_t closed_triangles;
+} hm_timings_t;
+int hm_graph_timings(const hm_graph* g, hm_timings_t* t);
+
+/* Class of a 7-bit region pattern: static class 0..29 or temporal motif
+ * 0..95 (-1 if the pattern is not a connected triple). Bits: exclusive parts
+ * of x, y, z; x&y only; y&z only; z&x only; x&y&z. */
+int hm_classify_static(int pattern);
+int hm_classify_temporal(int pattern);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,186 @@
+// C ABI entry points for graphs: build, destroy, info, query, static counts.
+#include <cstring>
+#include <mutex>
+
+#include "hm_classes.h"
+#include "hm_device.h"
+
+namespace {
+
+constexpr unsigned kBlock = 256;
+
+__global__ void k_query_sizes(const uint32_t* ids, uint32_t n, uint32_t n_slots, const uint32_t* live_bits,
+                              const uint32_t* h2v_len, uint32_t* sizes, int* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = ids[i];
+    if (id >= n_slots || !((live_bits[id >> 5] >> (id & 31)) & 1u)) {
+      atomicExch(bad, 1);
+      sizes[i] = 0;
+    } else {
+      sizes[i] = h2v_len[id];
+    }
+  }
+}
+
+__global__ void k_query_gather(const uint32_t* ids, uint32_t n, const uint64_t* out_off, const uint64_t* h2v_off,
+                               const uint32_t* h2v_mem, uint32_t* out) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint64_t i = warp; i < n; i += nw) {
+    const uint64_t d = out_off[i], len = out_off[i + 1] - d;
+    const uint64_t s = h2v_off[ids[i]];
+    for (uint64_t k = lane; k < len; k += 32) out[d + k] = h2v_mem[s + k];
+  }
+}
+
+struct CtxLock {
+  std::lock_guard<std::mutex> g;
+  explicit CtxLock(hm_ctx* c) : g(c->mu) { cudaSetDevice(c->device); }
+};
+
+}  // namespace
+
+extern "C" int hm_graph_build(hm_ctx* ctx, const uint64_t* offsets, const uint32_t* members, uint32_t n_edges,
+                              uint32_t n_nodes, const int64_t* timestamps, hm_graph** out) {
+  if (!ctx || !out || (n_edges && !offsets) || (n_edges && offsets[n_edges] && !members))
+    return hm::set_error(HM_ERR_INVALID, "hm_graph_build: NULL argument");
+  *out = nullptr;
+  if (n_edges && offsets[0] != 0) return hm::set_error(HM_ERR_INVALID, "hm_graph_build: offsets[0] must be 0");
+  CtxLock lock(ctx);
+  auto* g = new hm_graph();
+  g->ctx = ctx;
+  g->n_nodes = n_nodes;
+  static const uint64_t zero_off = 0;
+  const uint64_t* off = n_edges ? offsets : &zero_off;
+  int s = hm::build_h2v(g, off, members, n_edges);
+  if (s >= 0) s = hm::build_v2h(g);
+  if (s >= 0) s = hm::build_h2h_rows(g);
+  if (s >= 0 && timestamps) {
+    s = g->ts.alloc(ctx, n_edges);
+    if (s >= 0 && n_edges) {
+      cudaError_t e = cudaMemcpyAsync(g->ts.p, timestamps, sizeof(int64_t) * n_edges, cudaMemcpyHostToDevice, ctx->stream);
+      if (e != cudaSuccess) s = hm::set_error(HM_ERR_CUDA, "timestamps upload: %s", cudaGetErrorString(e));
+    }
+    g->temporal = true;
+  }
+  if (s >= 0) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) s = hm::set_error(HM_ERR_CUDA, "hm_graph_build: %s", cudaGetErrorString(e));
+  }
+  if (s < 0) {
+    delete g;
+    return s;
+  }
+  *out = g;
+  return HM_OK;
+}
+
+extern "C" int hm_graph_destroy(hm_graph* g) {
+  if (!g) return HM_OK;
+  hm_ctx* ctx = g->ctx;
+  {
+    CtxLock lock(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    delete g;
+  }
+  return HM_OK;
+}
+
+extern "C" int hm_graph_info(const hm_graph* g, hm_graph_info_t* info) {
+  if (!g || !info) return hm::set_error(HM_ERR_INVALID, "hm_graph_info: NULL argument");
+  std::memset(info, 0, sizeof(*info));
+  info->n_slots = g->n_slots;
+  info->n_live = g->n_live;
+  info->n_nodes = g->n_nodes;
+  info->n_members = g->h2v_tail;
+  info->n_adjacent = g->h2h_nnz;
+  info->n_oriented = g->plus_valid ? g->plus_nnz : 0;
+  info->device_bytes = g->ctx->used.load();
+  info->temporal = g->temporal ? 1 : 0;
+  return HM_OK;
+}
+
+extern "C" int hm_graph_timings(const hm_graph* g, hm_timings_t* t) {
+  if (!g || !t) return hm::set_error(HM_ERR_INVALID, "hm_graph_timings: NULL argument");
+  t->open_ms = g->times.open_ms;
+  t->closed_ms = g->times.closed_ms;
+  t->count_ms = g->times.total_ms;
+  t->update_ms = g->times.update_ms;
+  t->temporal_ms = g->times.temporal_ms;
+  t->closed_triangles = g->times.closed_triangles;
+  return HM_OK;
+}
+
+extern "C" int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]) {
+  if (!g || !out30) return hm::set_error(HM_ERR_INVALID, "hm_count_static30: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::count_static30(g, 0, 1, out30);
+}
+
+extern "C" int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_shards,
+                                       uint64_t out30[HM_N_STATIC_CLASSES]) {
+  if (!g || !out30) return hm::set_error(HM_ERR_INVALID, "hm_count_static30_shard: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::count_static30(g, shard, n_shards, out30);
+}
+
+extern "C" int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]) {
+  if (!g || !out26) return hm::set_error(HM_ERR_INVALID, "hm_count_static: NULL argument");
+  uint64_t c30[30];
+  CtxLock lock(g->ctx);
+  HM_TRY(hm::count_static30(g, 0, 1, c30));
+  int m = 0;
+  for (int k = 0; k < 30; ++k)
+    if (hm::static_class_reported(k)) out26[m++] = c30[k];
+  return HM_OK;
+}
+
+extern "C" int hm_graph_query(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t* offsets_out,
+                              uint32_t* members_out, size_t members_cap) {
+  if (!g || (n && (!ids || !offsets_out))) return hm::set_error(HM_ERR_INVALID, "hm_graph_query: NULL argument");
+  CtxLock lock(g->ctx);
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  offsets_out[0] = 0;
+  if (!n) return HM_OK;
+  hm::DArr<uint32_t> d_ids, sizes, d_out;
+  hm::DArr<uint64_t> d_off;
+  hm::DArr<int> bad;
+  HM_TRY(d_ids.alloc(ctx, n));
+  HM_TRY(sizes.alloc(ctx, n));
+  HM_TRY(d_off.alloc(ctx, (size_t)n + 1));
+  HM_TRY(bad.alloc(ctx, 1));
+  HM_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+  HM_CUDA(cudaMemcpyAsync(d_ids.p, ids, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+  k_query_sizes<<<hm::grid_for(n, kBlock), kBlock, 0, st>>>(d_ids.p, n, g->n_slots, g->live_bits.p, g->h2v_len.p,
+                                                           sizes.p, bad.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(hm::exclusive_scan(ctx, sizes.p, d_off.p, n));
+  int hbad = 0;
+  HM_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaMemcpyAsync(offsets_out, d_off.p, sizeof(uint64_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  if (hbad) return hm::set_error(HM_ERR_NOT_LIVE, "hm_graph_query: an id is not a live hyperedge");
+  const uint64_t total = offsets_out[n];
+  if (total > members_cap)
+    return hm::set_error(HM_ERR_CAPACITY, "hm_graph_query: %llu members > capacity %zu", (unsigned long long)total,
+                         members_cap);
+  if (!total) return HM_OK;
+  if (!members_out) return hm::set_error(HM_ERR_INVALID, "hm_graph_query: members_out is NULL");
+  HM_TRY(d_out.alloc(ctx, total));
+  k_query_gather<<<hm::grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(d_ids.p, n, d_off.p, g->h2v_off.p,
+                                                                           g->h2v_mem.p, d_out.p);
+  HM_LAUNCH_CHECK();
+  HM_CUDA(cudaMemcpyAsync(members_out, d_out.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  return HM_OK;
+}
+
+extern "C" int hm_classify_static(int pattern) { return hm::static_class_of_pattern(pattern & 127); }
+
+extern "C" int hm_classify_temporal(int pattern) {
+  for (int m = 0; m < HM_N_TEMPORAL_MOTIFS; ++m)
+    if (hm::kTemporalMotifPattern[m] == (pattern & 127)) return m;
+  return -1;
+}

@@ -1,0 +1,178 @@
+// Engine internals shared by the CUDA translation units: the context, device
+// arrays with budget accounting, the graph store, and error helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "hm_internal.h"
+
+#define HM_CUDA(call)                                                                                  \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess)                                                                             \
+      return ::hm::set_error(HM_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define HM_TRY(expr)          \
+  do {                        \
+    int s_ = (expr);          \
+    if (s_ < 0) return s_;    \
+  } while (0)
+
+#define HM_LAUNCH_CHECK() HM_CUDA(cudaGetLastError())
+
+struct hm_ctx {
+  int device = 0;
+  size_t budget = 0;  // bytes; 0 = all free memory at creation
+  std::atomic<size_t> used{0};
+  cudaStream_t stream = nullptr;
+  int n_sms = 148;
+  std::mutex mu;  // serialises calls that share this context
+};
+
+namespace hm {
+
+int dev_alloc(hm_ctx* ctx, void** p, size_t bytes);
+void dev_free(hm_ctx* ctx, void* p, size_t bytes);
+
+// Owning device array; the context's budget is charged for its bytes.
+template <class T>
+struct DArr {
+  hm_ctx* ctx = nullptr;
+  T* p = nullptr;
+  size_t n = 0;
+  DArr() = default;
+  DArr(const DArr&) = delete;
+  DArr& operator=(const DArr&) = delete;
+  DArr(DArr&& o) noexcept { *this = static_cast<DArr&&>(o); }
+  DArr& operator=(DArr&& o) noexcept {
+    if (this != &o) {
+      release();
+      ctx = o.ctx; p = o.p; n = o.n;
+      o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
+  ~DArr() { release(); }
+  int alloc(hm_ctx* c, size_t count) {
+    release();
+    ctx = c;
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    HM_TRY(dev_alloc(c, &q, count * sizeof(T)));
+    p = static_cast<T*>(q);
+    n = count;
+    return HM_OK;
+  }
+  void release() {
+    if (p) dev_free(ctx, p, n * sizeof(T));
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Per-phase device times of the last count call (CUDA events on the
+// context stream), reported through hm_graph_timings().
+struct PhaseTimes {
+  float open_ms = 0, closed_ms = 0, total_ms = 0, update_ms = 0, temporal_ms = 0;
+  uint64_t closed_triangles = 0;
+};
+
+}  // namespace hm
+
+// The device-resident hypergraph. Three segment tables share one layout:
+// key k owns entries [off[k], off[k] + len[k]) of its arena.
+//   H2V  hyperedge slot -> sorted member node ids (u32)
+//   V2H  node          -> sorted hyperedge slots (u32)
+//   H2H  hyperedge slot -> sorted adjacent slots (u32), overlap size (u8),
+//                          and the shared positions of the row owner's
+//                          member list as a bit mask (u64, positions < 64)
+// plus the oriented copy of H2H used by the triangle phase (neighbours of
+// higher (degree, id) rank only), and per-slot sizes and liveness.
+struct hm_graph {
+  hm_ctx* ctx = nullptr;
+  uint32_t n_slots = 0;  // ids 0..n_slots-1 (live or free)
+  uint32_t n_nodes = 0;
+  uint32_t n_live = 0;
+  uint32_t cap_slots = 0;
+
+  hm::DArr<uint8_t> esize;      // per slot, 0 for free slots
+  hm::DArr<uint32_t> live_bits; // one bit per slot
+
+  hm::DArr<uint64_t> h2v_off;
+  hm::DArr<uint32_t> h2v_len;
+  hm::DArr<uint32_t> h2v_mem;
+  uint64_t h2v_tail = 0;
+
+  hm::DArr<uint64_t> v2h_off;
+  hm::DArr<uint32_t> v2h_len;
+  hm::DArr<uint32_t> v2h_edge;
+  uint64_t v2h_tail = 0;
+
+  hm::DArr<uint64_t> h2h_off;
+  hm::DArr<uint32_t> h2h_len;
+  hm::DArr<uint32_t> h2h_nbr;
+  hm::DArr<uint8_t> h2h_ovl;
+  hm::DArr<uint64_t> h2h_mask;
+  uint64_t h2h_tail = 0;
+  uint64_t h2h_nnz = 0;
+
+  // oriented adjacency (rebuilt lazily after updates)
+  bool plus_valid = false;
+  hm::DArr<uint64_t> plus_off;
+  hm::DArr<uint32_t> plus_len;
+  hm::DArr<uint32_t> plus_nbr;
+  hm::DArr<uint16_t> plus_os;  // (neighbour size << 8) | overlap
+  hm::DArr<uint64_t> plus_mask;
+  uint64_t plus_nnz = 0;
+
+  // static-count state that only changes with the graph
+  bool work_valid = false;
+  hm::DArr<uint32_t> work;  // centres owning oriented wedges, heaviest first
+  uint32_t n_work = 0;
+  hm::DArr<unsigned long long> counters;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  bool ev_ready = false;
+
+  // temporal (optional): timestamps per slot
+  hm::DArr<int64_t> ts;
+  bool temporal = false;
+
+  hm::PhaseTimes times;
+
+  ~hm_graph() {
+    if (ev_ready)
+      for (auto& e : ev) cudaEventDestroy(e);
+  }
+};
+
+namespace hm {
+
+// Store construction pieces (hm_store.cu).
+int build_h2v(hm_graph* g, const uint64_t* h_off, const uint32_t* h_mem, uint32_t n_edges);
+int build_v2h(hm_graph* g);
+int build_h2h_rows(hm_graph* g);
+int build_plus(hm_graph* g);
+template <class T>
+int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n);
+
+// Static count (hm_static.cu).
+int prepare_static(hm_graph* g);
+int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags);
+int finish_static(hm_graph* g, uint64_t out30[30]);
+int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
+
+inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
+  uint64_t b = (items + per_block - 1) / per_block;
+  if (b == 0) b = 1;
+  return (unsigned)(b < max_blocks ? b : max_blocks);
+}
+
+}  // namespace hm

@@ -1,0 +1,478 @@
+// Exact static h-motif counting (the 30 classes behind MoCHy's 26 motifs).
+//
+// Reference semantics: MoCHy exact (MoCHy-master/main_exact.cpp:91-129)
+// classifies every connected triple {a, b, c} of distinct hyperedges: open
+// triples (exactly two overlapping pairs) at their centre, closed triples once.
+// The reference GPU counter (dynamicHyperGraph/src/HMotifCount.cu:16-125) runs
+// one thread per hyperedge over closed triangles only and never sees open
+// triples; this file counts both.
+//
+// Algorithm (all integer, exact):
+//   1. Open phase, one warp per centre a. Every unordered neighbour pair
+//      {b, c} of a is classified as if it were open: its class depends only on
+//      [C_ab + C_ac < |a|], [C_ab < |b|], [C_ac < |c|]. A histogram of the
+//      neighbours by (overlap, [overlap < size]) gives the six class counts
+//      with prefix sums, without touching pairs one by one.
+//   2. Closed phase, one block per centre a (the lowest-ranked corner under
+//      (degree, id) order): N+(a) goes into a shared-memory hash table, each
+//      warp walks N+(b) for one b in N+(a) and probes it. Every triangle is
+//      found exactly once; it adds its closed class and removes the three
+//      open-pair classes phase 1 gave it at its three centres.
+//   The triple overlap g = |a & b & c| is popc(mask_ab & mask_ac), where each
+//   adjacency entry carries the positions of the owner's members it shares;
+//   centres with more than 64 members fall back to a merge of the lists.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "hm_classes.h"
+#include "hm_device.h"
+
+namespace hm {
+
+namespace {
+
+constexpr unsigned kWarp = 32;
+constexpr unsigned kOpenBlock = 256;
+constexpr unsigned kOpenWarps = kOpenBlock / kWarp;
+constexpr unsigned kClosedBlock = 256;
+constexpr unsigned kClosedWarps = kClosedBlock / kWarp;
+constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair classes
+constexpr unsigned kHashSlotsMax = 8192;     // shared-memory hash table capacity
+constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint64_t global_warp() { return ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint64_t n_warps() { return ((uint64_t)gridDim.x * blockDim.x) >> 5; }
+
+__device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
+  for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  return v;
+}
+
+// ---- phase 1: all neighbour pairs of each centre, classified as open --------
+
+__global__ void __launch_bounds__(kOpenBlock) k_open_pairs(const uint64_t* __restrict__ off,
+                                                           const uint32_t* __restrict__ len,
+                                                           const uint32_t* __restrict__ nbr,
+                                                           const uint8_t* __restrict__ ovl,
+                                                           const uint8_t* __restrict__ esize, uint32_t n,
+                                                           uint32_t shard, uint32_t n_shards,
+                                                           unsigned long long* __restrict__ out6) {
+  __shared__ uint32_t hist[kOpenWarps][2][256];
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  uint64_t acc[6] = {0, 0, 0, 0, 0, 0};  // lane 0's running class counts
+  for (uint64_t a = shard + global_warp() * n_shards; a < n; a += n_warps() * n_shards) {
+    const uint32_t l = len[a];
+    if (l < 2) continue;
+    const uint32_t s = esize[a];
+    for (uint32_t i = lane; i <= s; i += kWarp) {
+      hist[w][0][i] = 0;
+      hist[w][1][i] = 0;
+    }
+    __syncwarp();
+    const uint64_t base = off[a];
+    uint32_t one[2] = {0, 0};  // overlap-1 neighbours, the common case, kept in registers
+    for (uint32_t i = lane; i < l; i += kWarp) {
+      const uint32_t b = nbr[base + i];
+      const uint32_t c = ovl[base + i];
+      const uint32_t y = c < esize[b];
+      if (c == 1) ++one[y];
+      else atomicAdd(&hist[w][y][c], 1u);
+    }
+    for (int d = 16; d; d >>= 1) {
+      one[0] += __shfl_xor_sync(0xffffffffu, one[0], d);
+      one[1] += __shfl_xor_sync(0xffffffffu, one[1], d);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      uint32_t* h0 = hist[w][0];
+      uint32_t* h1 = hist[w][1];
+      h0[1] += one[0];
+      h1[1] += one[1];
+      // in-place prefix sums: H_t[k] = #neighbours of type t with overlap <= k
+      for (uint32_t k = 1; k <= s; ++k) {
+        h0[k] += h0[k - 1];
+        h1[k] += h1[k - 1];
+      }
+      const uint64_t n0 = h0[s], n1 = h1[s];
+      // ordered pairs (b, c), b of type t, c of type u, with C_b + C_c <= s - 1
+      uint64_t l00 = 0, l01 = 0, l11 = 0, d0 = 0, d1 = 0;
+      for (uint32_t c1 = 1; c1 + 1 < s; ++c1) {
+        const uint64_t x0 = h0[c1] - h0[c1 - 1], x1 = h1[c1] - h1[c1 - 1];
+        const uint32_t m = s - 1 - c1;
+        l00 += x0 * h0[m];
+        l01 += x0 * h1[m];
+        l11 += x1 * h1[m];
+        if (2 * c1 <= s - 1) {
+          d0 += x0;
+          d1 += x1;
+        }
+      }
+      const uint64_t p00 = (l00 - d0) / 2, p11 = (l11 - d1) / 2, p01 = l01;
+      const uint64_t t00 = n0 * (n0 - (n0 > 0)) / 2, t11 = n1 * (n1 - (n1 > 0)) / 2, t01 = n0 * n1;
+      // open class index = x + 2 * (#ends with an exclusive part)
+      acc[1] += p00;
+      acc[0] += t00 - p00;
+      acc[3] += p01;
+      acc[2] += t01 - p01;
+      acc[5] += p11;
+      acc[4] += t11 - p11;
+    }
+    __syncwarp();
+  }
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k)
+      if (acc[k]) atomicAdd(&out6[k], (unsigned long long)acc[k]);
+}
+
+// ---- phase 2: closed triangles ------------------------------------------------
+
+struct ClosedArgs {
+  const uint64_t* poff;
+  const uint32_t* plen;
+  const uint32_t* pnbr;
+  const uint16_t* pos;    // (neighbour size << 8) | overlap
+  const uint64_t* pmask;  // shared positions of the row owner's members (< 64)
+  const uint64_t* hoff;   // H2V
+  const uint32_t* hmem;
+  const uint8_t* esize;
+  const uint32_t* work;  // centres, heaviest first
+  uint32_t n_work;
+  uint32_t shard, n_shards;  // this call takes work items shard, shard + n_shards, ...
+  unsigned int* queue;
+  unsigned long long* out;  // kNumCounters
+  uint8_t* edge_flags;      // diagnostics only: marks oriented entries that close a triangle
+};
+
+// |a & b & c| by a three-way merge of the member lists (centres with more
+// than 64 members, whose position masks are incomplete).
+__device__ uint32_t triple_overlap(const uint64_t* hoff, const uint32_t* hmem, const uint8_t* esize, uint32_t a,
+                                   uint32_t b, uint32_t c) {
+  const uint32_t* x = hmem + hoff[a];
+  const uint32_t* y = hmem + hoff[b];
+  const uint32_t* z = hmem + hoff[c];
+  const uint32_t nx = esize[a], ny = esize[b], nz = esize[c];
+  uint32_t i = 0, j = 0, k = 0, g = 0;
+  while (i < nx && j < ny && k < nz) {
+    const uint32_t u = x[i], v = y[j], t = z[k];
+    const uint32_t m = max(u, max(v, t));
+    if (u == m && v == m && t == m) {
+      ++g; ++i; ++j; ++k;
+    } else {
+      i += (u < m);
+      j += (v < m);
+      k += (t < m);
+    }
+  }
+  return g;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t key, uint32_t shift) { return (key * 2654435761u) >> shift; }
+
+// Size category used by the star fast path: 0 for |x| = 1, 1 for |x| = 2, 2
+// for |x| >= 3 (the classes of a star triple only depend on these).
+__device__ __forceinline__ uint32_t size_cat(uint32_t s) { return s >= 3 ? 2u : s - 1u; }
+
+// Adds n triangles {a, b, c} whose three pairs share exactly one node, the
+// same one (g = 1), with size categories ca, cb, cc: closed class = number of
+// members with |x| >= 2; open-pair classes at each centre x as phase 1 gave
+// them: [|x| >= 3] + 2 ([|y| >= 2] + [|z| >= 2]).
+__device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, uint32_t cb, uint32_t cc,
+                                         uint64_t n) {
+  const uint32_t ea = ca > 0, eb = cb > 0, ec = cc > 0;
+  wc[ea + eb + ec] += n;
+  wc[30 + (ca == 2) + 2 * (eb + ec)] += n;
+  wc[30 + (cb == 2) + 2 * (ea + ec)] += n;
+  wc[30 + (cc == 2) + 2 * (ea + eb)] += n;
+}
+
+// One block per centre a (the lowest-ranked corner of its triangles). The
+// oriented row N+(a) goes into a shared-memory hash table (load <= 1/4 for
+// rows up to 2048) with each entry's overlap and shared-position mask; each
+// warp takes one b in N+(a) and its lanes probe N+(b). For a centre with at
+// most 64 members, g = |a & b & c| = popc(mask_ab & mask_ac) exactly. Star
+// triangles (all three overlaps 1, the same shared node) are only counted
+// per size category in registers; the others are classified and their four
+// counter updates aggregated across the lanes that share them.
+__global__ void __launch_bounds__(kClosedBlock, 2) k_closed(ClosedArgs A) {
+  extern __shared__ uint64_t smem64[];
+  uint64_t* smask = smem64;                                            // kHashSlotsMax
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kHashSlotsMax); // kHashSlotsMax
+  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kHashSlotsMax);    // kHashSlotsMax
+  __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
+  __shared__ uint32_t s_item;
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  unsigned long long* wc = wcnt[w];
+  for (unsigned k = lane; k < kNumCounters; k += kWarp) wc[k] = 0;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1u);
+    __syncthreads();
+    const uint64_t item = (uint64_t)s_item * A.n_shards + A.shard;
+    if (item >= A.n_work) break;
+    const uint32_t a = A.work[item];
+    const uint64_t ao = A.poff[a];
+    const uint32_t ad = A.plen[a];
+    const uint32_t sa = A.esize[a];
+    const bool in_smem = ad <= kHashRowMax;
+    const bool flags = A.edge_flags != nullptr;
+    uint32_t shift = 32, mask = 0;
+    if (in_smem) {
+      uint32_t slots = 64;
+      while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
+      shift = 32 - (31 - __clz(slots));
+      mask = slots - 1;
+      for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < ad; i += blockDim.x) {
+        const uint32_t key = A.pnbr[ao + i];
+        uint32_t h = hash_slot(key, shift);
+        while (atomicCAS(&keys[h], kEmpty, key) != kEmpty) h = (h + 1) & mask;
+        smask[h] = flags ? (uint64_t)i : A.pmask[ao + i];  // diagnostics keep the row index
+        sovl[h] = (uint8_t)(A.pos[ao + i] & 0xffu);
+      }
+    }
+    __syncthreads();
+    const uint32_t cat_a = size_cat(sa);
+    const bool exact_masks = sa <= 64;
+    for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
+      const uint32_t b = A.pnbr[ao + bi];
+      const uint32_t osb = A.pos[ao + bi];
+      const uint32_t cab = osb & 0xffu, sb = osb >> 8;
+      const uint64_t mab = A.pmask[ao + bi];
+      const uint64_t bo = A.poff[b];
+      const uint32_t bd = A.plen[b];
+      uint32_t star0 = 0, star1 = 0, star2 = 0;
+      for (uint32_t j = lane; j < bd; j += kWarp) {
+        const uint32_t c = A.pnbr[bo + j];
+        uint32_t cac = 0;
+        uint64_t mac = 0;
+        if (in_smem) {
+          uint32_t h = hash_slot(c, shift);
+          uint32_t k = keys[h];
+          while (k != c && k != kEmpty) {
+            h = (h + 1) & mask;
+            k = keys[h];
+          }
+          if (k == c) {
+            cac = sovl[h];
+            mac = smask[h];
+            if (flags) {
+              A.edge_flags[ao + mac] = 1;
+              A.edge_flags[ao + bi] = 1;
+              A.edge_flags[bo + j] = 1;
+              mac = A.pmask[ao + mac];
+            }
+          }
+        } else {
+          uint32_t lo = 0, hi = ad;
+          const uint32_t* row = A.pnbr + ao;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (row[mid] < c) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo < ad && row[lo] == c) {
+            cac = A.pos[ao + lo] & 0xffu;
+            mac = A.pmask[ao + lo];
+            if (flags) {
+              A.edge_flags[ao + lo] = 1;
+              A.edge_flags[ao + bi] = 1;
+              A.edge_flags[bo + j] = 1;
+            }
+          }
+        }
+        if (!cac) continue;
+        const uint32_t osc = A.pos[bo + j];
+        const uint32_t cbc = osc & 0xffu, sc = osc >> 8;
+        uint32_t g;
+        if (exact_masks) {
+          if ((cab | cac | cbc) == 1 && mab == mac) {
+            const uint32_t cc = size_cat(sc);
+            star0 += cc == 0;
+            star1 += cc == 1;
+            star2 += cc == 2;
+            continue;
+          }
+          g = __popcll(mab & mac);
+        } else {
+          g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
+        }
+        const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
+        if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+        // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
+        const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
+        const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
+        const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
+        const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
+        const unsigned peers = __match_any_sync(__activemask(), key);
+        if (lane == (unsigned)(__ffs(peers) - 1)) {
+          const unsigned long long n = (unsigned long long)__popc(peers);
+          atomicAdd(&wc[k], n);
+          atomicAdd(&wc[30 + oa], n);
+          atomicAdd(&wc[30 + ob], n);
+          atomicAdd(&wc[30 + oc], n);
+        }
+      }
+      if (cab == 1 && exact_masks) {
+        for (int d = 16; d; d >>= 1) {
+          star0 += __shfl_xor_sync(0xffffffffu, star0, d);
+          star1 += __shfl_xor_sync(0xffffffffu, star1, d);
+          star2 += __shfl_xor_sync(0xffffffffu, star2, d);
+        }
+        if (lane == 0) {
+          const uint32_t cat_b = size_cat(sb);
+          if (star0) add_star(wc, cat_a, cat_b, 0, star0);
+          if (star1) add_star(wc, cat_a, cat_b, 1, star1);
+          if (star2) add_star(wc, cat_a, cat_b, 2, star2);
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  __syncwarp();
+  for (unsigned k = lane; k < kNumCounters; k += kWarp)
+    if (wc[k]) atomicAdd(&A.out[k], wc[k]);
+}
+
+// Work estimate per centre: sum of d+(b) over b in N+(a); centres with fewer
+// than two oriented neighbours own no triangle and are dropped.
+__global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, uint32_t n,
+                              uint64_t* est, uint32_t* ids) {
+  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+    const uint32_t d = plen[a];
+    uint64_t s = 0;
+    if (d >= 2)
+      for (uint32_t i = lane_id(); i < d; i += kWarp) s += plen[pnbr[poff[a] + i]];
+    s = warp_sum(s);
+    if (lane_id() == 0) {
+      est[a] = (d >= 2 && s > 0) ? s + d : 0;
+      ids[a] = (uint32_t)a;
+    }
+  }
+}
+
+}  // namespace
+
+size_t closed_smem_bytes() { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * kHashSlotsMax; }
+
+// Centres that own at least one oriented wedge, heaviest first.
+static int closed_worklist(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  DArr<uint64_t> est, est_sorted;
+  DArr<uint32_t> ids;
+  HM_TRY(est.alloc(ctx, E));
+  HM_TRY(est_sorted.alloc(ctx, E));
+  HM_TRY(ids.alloc(ctx, E));
+  HM_TRY(g->work.alloc(ctx, E));
+  k_closed_work<<<grid_for((uint64_t)E * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p, E,
+                                                                est.p, ids.p);
+  HM_LAUNCH_CHECK();
+  size_t tb = 0;
+  HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, g->work.p, (int64_t)E,
+                                                    0, 64, st));
+  DArr<uint8_t> tmp;
+  HM_TRY(tmp.alloc(ctx, tb));
+  HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, est.p, est_sorted.p, ids.p, g->work.p, (int64_t)E, 0,
+                                                    64, st));
+  // the number of non-zero estimates is the first zero of the descending list
+  std::vector<uint64_t> h(E);
+  HM_CUDA(cudaMemcpyAsync(h.data(), est_sorted.p, sizeof(uint64_t) * E, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  uint32_t lo = 0, hi = E;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (h[mid] > 0) lo = mid + 1;
+    else hi = mid;
+  }
+  g->n_work = lo;
+  g->work_valid = true;
+  return HM_OK;
+}
+
+// Everything the count kernels need that only changes with the graph.
+int prepare_static(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  if (!g->plus_valid) {
+    HM_TRY(build_plus(g));
+    g->work_valid = false;
+  }
+  if (!g->work_valid && g->n_slots) HM_TRY(closed_worklist(g));
+  if (!g->counters.p) HM_TRY(g->counters.alloc(ctx, 64));
+  if (!g->ev_ready) {
+    for (auto& e : g->ev) HM_CUDA(cudaEventCreate(&e));
+    g->ev_ready = true;
+  }
+  static bool attr_set = false;
+  if (!attr_set) {
+    HM_CUDA(cudaFuncSetAttribute(k_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)closed_smem_bytes()));
+    attr_set = true;
+  }
+  return HM_OK;
+}
+
+// Launches both phases for one shard of the centres; the counters land in
+// g->counters ([0,30) closed classes, [30,36) open-pair removals, [36,42)
+// open-pair counts, [42] work queue). edge_flags is for diagnostics.
+int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  unsigned long long* dev = g->counters.p;
+  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 43, st));
+  HM_CUDA(cudaEventRecord(g->ev[0], st));
+  if (E) {
+    k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                 g->h2h_ovl.p, g->esize.p, E, shard, n_shards,
+                                                                 dev + 36);
+    HM_LAUNCH_CHECK();
+  }
+  HM_CUDA(cudaEventRecord(g->ev[1], st));
+  if (g->n_work > shard) {
+    ClosedArgs A{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p,
+                 g->esize.p, g->work.p, g->n_work, shard, n_shards, reinterpret_cast<unsigned int*>(dev + 42), dev,
+                 edge_flags};
+    const uint32_t items = (g->n_work - shard + n_shards - 1) / n_shards;
+    const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
+    k_closed<<<grid, kClosedBlock, closed_smem_bytes(), st>>>(A);
+    HM_LAUNCH_CHECK();
+  }
+  HM_CUDA(cudaEventRecord(g->ev[2], st));
+  return HM_OK;
+}
+
+int finish_static(hm_graph* g, uint64_t out30[30]) {
+  unsigned long long h[43];
+  cudaStream_t st = g->ctx->stream;
+  HM_CUDA(cudaMemcpyAsync(h, g->counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  float t_open = 0, t_closed = 0;
+  cudaEventElapsedTime(&t_open, g->ev[0], g->ev[1]);
+  cudaEventElapsedTime(&t_closed, g->ev[1], g->ev[2]);
+  g->times.open_ms = t_open;
+  g->times.closed_ms = t_closed;
+  g->times.total_ms = t_open + t_closed;
+  uint64_t tri = 0;
+  for (int k = 0; k < 30; ++k) {
+    out30[k] = h[k];
+    tri += h[k];
+  }
+  for (int k = 0; k < 6; ++k) out30[20 + k] += h[36 + k] - h[30 + k];
+  g->times.closed_triangles = tri;
+  return HM_OK;
+}
+
+int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]) {
+  if (n_shards == 0 || shard >= n_shards) return set_error(HM_ERR_INVALID, "static count: shard %u of %u", shard, n_shards);
+  HM_TRY(prepare_static(g));
+  HM_TRY(launch_static(g, shard, n_shards, nullptr));
+  return finish_static(g, out30);
+}
+
+}  // namespace hm

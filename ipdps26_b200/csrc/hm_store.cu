@@ -1,0 +1,550 @@
+// Device-resident hypergraph store: construction of H2V, V2H, H2H (with
+// overlap sizes and smallest shared node) and the oriented adjacency.
+//
+// Reference counterpart: constructCBST / CBSTOperations::construct
+// (dynamicHyperGraph/structure/operations.cu:31-80, 412-415) and the host
+// adjacency builder hyperedgeAdjacency (dynamicHyperGraph/utils/utils.cpp:
+// 399-427). There, keys 1..N sit in a level-order BST whose nodes point into
+// a padded int payload and H2H is built on the host with std::set and no
+// overlap sizes. Here ids are dense, so a direct id -> (offset, length)
+// segment table replaces the tree walk; every table is built on the device
+// by sort / scan / compact kernels.
+#include <cub/cub.cuh>
+#include <thrust/iterator/transform_iterator.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "hm_device.h"
+
+namespace hm {
+
+namespace {
+
+constexpr unsigned kWarp = 32;
+constexpr unsigned kBlock = 256;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+__device__ __forceinline__ uint64_t global_warp() { return ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint64_t n_warps() { return ((uint64_t)gridDim.x * blockDim.x) >> 5; }
+
+// ---- H2V normalisation ----------------------------------------------------
+
+__global__ void k_seg_bounds(const uint64_t* off, uint32_t n, int* beg, int* end) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+    beg[r] = (int)off[r];
+    end[r] = (int)off[r + 1];
+  }
+}
+
+// Distinct count of each sorted row; flags node ids >= n_nodes.
+__global__ void k_row_distinct(const uint64_t* off, const uint32_t* mem, uint32_t n, uint32_t n_nodes,
+                               uint32_t* cnt, int* bad) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint64_t s = off[r], e = off[r + 1];
+    uint32_t c = 0;
+    for (uint64_t i0 = s; i0 < e; i0 += kWarp) {
+      const uint64_t i = i0 + lane_id();
+      bool first = false;
+      if (i < e) {
+        const uint32_t v = mem[i];
+        if (v >= n_nodes) atomicExch(bad, 1);
+        first = (i == s) || (mem[i - 1] != v);
+      }
+      c += __popc(__ballot_sync(0xffffffffu, first));
+    }
+    if (lane_id() == 0) cnt[r] = c;
+  }
+}
+
+__global__ void k_row_distinct_write(const uint64_t* off, const uint32_t* mem, uint32_t n, const uint64_t* out_off,
+                                     uint32_t* out) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint64_t s = off[r], e = off[r + 1];
+    uint64_t w = out_off[r];
+    for (uint64_t i0 = s; i0 < e; i0 += kWarp) {
+      const uint64_t i = i0 + lane_id();
+      bool first = false;
+      uint32_t v = 0;
+      if (i < e) {
+        v = mem[i];
+        first = (i == s) || (mem[i - 1] != v);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, first);
+      if (first) out[w + __popc(m & lanemask_lt())] = v;
+      w += __popc(m);
+    }
+  }
+}
+
+__global__ void k_u32_to_u8_checked(const uint32_t* in, uint32_t n, uint8_t* out, uint32_t limit, int* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t v = in[i];
+    if (v > limit) atomicExch(bad, 1);
+    out[i] = (uint8_t)(v > 255 ? 255 : v);
+  }
+}
+
+__global__ void k_fill_live_bits(uint32_t* bits, uint32_t n_words, uint32_t n_live) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words; w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t lo = w * 32;
+    uint32_t v = 0;
+    if (lo + 32 <= n_live) v = 0xffffffffu;
+    else if (lo < n_live) v = (1u << (n_live - lo)) - 1u;
+    bits[w] = v;
+  }
+}
+
+// ---- V2H ---------------------------------------------------------------------
+
+// (node, slot) pairs in slot order, so a stable sort by node keeps slots
+// ascending within each node.
+__global__ void k_member_pairs(const uint64_t* off, const uint32_t* len, const uint32_t* mem, uint32_t n,
+                               uint32_t* keys, uint32_t* vals, uint32_t* node_cnt) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint64_t s = off[r];
+    const uint32_t l = len[r];
+    for (uint32_t i = lane_id(); i < l; i += kWarp) {
+      const uint32_t v = mem[s + i];
+      keys[s + i] = v;
+      vals[s + i] = (uint32_t)r;
+      atomicAdd(&node_cnt[v], 1u);
+    }
+  }
+}
+
+// ---- H2H ---------------------------------------------------------------------
+
+__global__ void k_wedge_count(const uint64_t* off, const uint32_t* len, const uint32_t* mem, const uint32_t* vlen,
+                              uint32_t n, uint64_t* wedges) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint64_t s = off[r];
+    const uint32_t l = len[r];
+    uint64_t w = 0;
+    for (uint32_t i = lane_id(); i < l; i += kWarp) w += vlen[mem[s + i]] - 1u;
+    for (int d = 16; d; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
+    if (lane_id() == 0) wedges[r] = w;
+  }
+}
+
+// Every (b, position of the shared node in r) for b != r sharing a node with
+// r, written as key (b << 8) | pos into r's range of the chunk buffer.
+__global__ void k_expand(const uint64_t* h_off, const uint32_t* h_len, const uint32_t* h_mem, const uint64_t* v_off,
+                         const uint32_t* v_len, const uint32_t* v_edge, const uint64_t* wedge_off,
+                         uint64_t chunk_base, uint32_t r0, uint32_t r1, uint32_t* keys) {
+  for (uint64_t r = r0 + global_warp(); r < r1; r += n_warps()) {
+    uint64_t pos = wedge_off[r] - chunk_base;
+    const uint64_t s = h_off[r];
+    const uint32_t l = h_len[r];
+    for (uint32_t p = 0; p < l; ++p) {
+      const uint32_t v = h_mem[s + p];
+      const uint64_t lo = v_off[v];
+      const uint32_t n = v_len[v];
+      for (uint32_t j0 = 0; j0 < n; j0 += kWarp) {
+        const uint32_t j = j0 + lane_id();
+        uint32_t b = 0;
+        bool keep = false;
+        if (j < n) {
+          b = v_edge[lo + j];
+          keep = (b != (uint32_t)r);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) keys[pos + __popc(m & lanemask_lt())] = (b << 8) | p;
+        pos += __popc(m);
+      }
+    }
+  }
+}
+
+__global__ void k_chunk_bounds(const uint64_t* wedge_off, uint64_t chunk_base, uint32_t r0, uint32_t r1, int* beg,
+                               int* end) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < r1 - r0; i += (uint64_t)gridDim.x * blockDim.x) {
+    beg[i] = (int)(wedge_off[r0 + i] - chunk_base);
+    end[i] = (int)(wedge_off[r0 + i + 1] - chunk_base);
+  }
+}
+
+// Number of distinct neighbours per row of a sorted chunk.
+__global__ void k_chunk_distinct(const int* beg, const int* end, const uint32_t* keys, uint32_t nrows, uint32_t* cnt) {
+  for (uint64_t r = global_warp(); r < nrows; r += n_warps()) {
+    const int s = beg[r], e = end[r];
+    uint32_t c = 0;
+    for (int i0 = s; i0 < e; i0 += kWarp) {
+      const int i = i0 + (int)lane_id();
+      bool first = false;
+      if (i < e) first = (i == s) || ((keys[i] >> 8) != (keys[i - 1] >> 8));
+      c += __popc(__ballot_sync(0xffffffffu, first));
+    }
+    if (lane_id() == 0) cnt[r] = c;
+  }
+}
+
+// Run starts (row-relative) of each row, at the row's local output offset.
+__global__ void k_chunk_starts(const int* beg, const int* end, const uint32_t* keys, uint32_t nrows,
+                               const uint64_t* local_off, uint32_t* starts) {
+  for (uint64_t r = global_warp(); r < nrows; r += n_warps()) {
+    const int s = beg[r], e = end[r];
+    uint64_t w = local_off[r];
+    for (int i0 = s; i0 < e; i0 += kWarp) {
+      const int i = i0 + (int)lane_id();
+      bool first = false;
+      if (i < e) first = (i == s) || ((keys[i] >> 8) != (keys[i - 1] >> 8));
+      const unsigned m = __ballot_sync(0xffffffffu, first);
+      if (first) starts[w + __popc(m & lanemask_lt())] = (uint32_t)(i - s);
+      w += __popc(m);
+    }
+  }
+}
+
+__global__ void k_chunk_emit(const int* beg, const int* end, const uint32_t* keys, uint32_t r0, uint32_t nrows,
+                             const uint64_t* local_off, const uint32_t* cnt, const uint32_t* starts,
+                             uint64_t out_base, uint64_t* row_off,
+                             uint32_t* row_len, uint32_t* nbr, uint8_t* ovl, uint64_t* pmask) {
+  for (uint64_t r = global_warp(); r < nrows; r += n_warps()) {
+    const int s = beg[r], e = end[r];
+    const uint64_t lo = local_off[r];
+    const uint32_t c = cnt[r];
+    const uint64_t dst = out_base + lo;
+    if (lane_id() == 0) {
+      row_off[r0 + r] = dst;
+      row_len[r0 + r] = c;
+    }
+    for (uint32_t k = lane_id(); k < c; k += kWarp) {
+      const uint32_t st = starts[lo + k];
+      const uint32_t en = (k + 1 < c) ? starts[lo + k + 1] : (uint32_t)(e - s);
+      const uint32_t key = keys[s + st];
+      nbr[dst + k] = key >> 8;
+      ovl[dst + k] = (uint8_t)(en - st);
+      uint64_t m = 0;
+      for (uint32_t q = st; q < en; ++q) {
+        const uint32_t pos = keys[s + q] & 255u;
+        if (pos < 64) m |= 1ull << pos;
+      }
+      pmask[dst + k] = m;
+    }
+  }
+}
+
+// ---- oriented adjacency --------------------------------------------------------
+
+// b is "above" a when (deg b, b) > (deg a, a): every triangle is found once,
+// from its lowest-ranked corner, and hub rows stay short.
+__device__ __forceinline__ bool above(uint32_t a, uint32_t da, uint32_t b, uint32_t db) {
+  return db > da || (db == da && b > a);
+}
+
+__global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, uint32_t n,
+                             uint32_t* cnt) {
+  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+    const uint64_t s = off[a];
+    const uint32_t l = len[a];
+    uint32_t c = 0;
+    for (uint32_t i0 = 0; i0 < l; i0 += kWarp) {
+      const uint32_t i = i0 + lane_id();
+      bool up = false;
+      if (i < l) {
+        const uint32_t b = nbr[s + i];
+        up = above((uint32_t)a, l, b, len[b]);
+      }
+      c += __popc(__ballot_sync(0xffffffffu, up));
+    }
+    if (lane_id() == 0) cnt[a] = c;
+  }
+}
+
+__global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint8_t* ovl,
+                             const uint64_t* mask, const uint8_t* esize, uint32_t n, const uint64_t* poff,
+                             uint32_t* pnbr, uint16_t* pos, uint64_t* pmask) {
+  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+    const uint64_t s = off[a];
+    const uint32_t l = len[a];
+    uint64_t w = poff[a];
+    for (uint32_t i0 = 0; i0 < l; i0 += kWarp) {
+      const uint32_t i = i0 + lane_id();
+      bool up = false;
+      uint32_t b = 0;
+      if (i < l) {
+        b = nbr[s + i];
+        up = above((uint32_t)a, l, b, len[b]);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, up);
+      if (up) {
+        const uint64_t d = w + __popc(m & lanemask_lt());
+        pnbr[d] = b;
+        pos[d] = (uint16_t)(((uint32_t)esize[b] << 8) | ovl[s + i]);
+        pmask[d] = mask[s + i];
+      }
+      w += __popc(m);
+    }
+  }
+}
+
+}  // namespace
+
+struct WidenU64 {
+  __host__ __device__ uint64_t operator()(uint32_t x) const { return x; }
+};
+
+// out[0..n]: exclusive prefix sums of in[0..n) with the total at out[n]; the
+// sum is accumulated in 64 bits whatever the input width.
+template <class T>
+int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n) {
+  HM_CUDA(cudaMemsetAsync(out, 0, sizeof(uint64_t), ctx->stream));
+  if (!n) return HM_OK;
+  size_t tb = 0;
+  if constexpr (sizeof(T) == 4) {
+    auto it = thrust::make_transform_iterator(in, WidenU64());
+    HM_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, it, out + 1, (int64_t)n, ctx->stream));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, it, out + 1, (int64_t)n, ctx->stream));
+  } else {
+    HM_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, in, out + 1, (int64_t)n, ctx->stream));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, in, out + 1, (int64_t)n, ctx->stream));
+  }
+  return HM_OK;
+}
+
+template int exclusive_scan<uint32_t>(hm_ctx*, const uint32_t*, uint64_t*, uint64_t);
+template int exclusive_scan<uint64_t>(hm_ctx*, const uint64_t*, uint64_t*, uint64_t);
+
+// Upload hyperedges, sort and deduplicate each member list on the device.
+int build_h2v(hm_graph* g, const uint64_t* h_off, const uint32_t* h_mem, uint32_t n_edges) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint64_t nnz = h_off[n_edges];
+  if (nnz >= (1ull << 31)) return set_error(HM_ERR_LIMIT, "hm_graph_build: %llu members exceed 2^31", (unsigned long long)nnz);
+  for (uint32_t e = 0; e < n_edges; ++e)
+    if (h_off[e + 1] < h_off[e]) return set_error(HM_ERR_INVALID, "hm_graph_build: offsets decrease at %u", e);
+  DArr<uint64_t> raw_off;
+  DArr<uint32_t> raw, sorted;
+  DArr<int> beg, end;
+  HM_TRY(raw_off.alloc(ctx, (size_t)n_edges + 1));
+  HM_TRY(raw.alloc(ctx, nnz));
+  HM_TRY(sorted.alloc(ctx, nnz));
+  HM_TRY(beg.alloc(ctx, n_edges));
+  HM_TRY(end.alloc(ctx, n_edges));
+  HM_CUDA(cudaMemcpyAsync(raw_off.p, h_off, sizeof(uint64_t) * ((size_t)n_edges + 1), cudaMemcpyHostToDevice, st));
+  if (nnz) HM_CUDA(cudaMemcpyAsync(raw.p, h_mem, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, st));
+  if (n_edges) {
+    k_seg_bounds<<<grid_for(n_edges, kBlock), kBlock, 0, st>>>(raw_off.p, n_edges, beg.p, end.p);
+    HM_LAUNCH_CHECK();
+  }
+  if (nnz) {
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, raw.p, sorted.p, (int)nnz, (int)n_edges, beg.p, end.p, st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp.p, tb, raw.p, sorted.p, (int)nnz, (int)n_edges, beg.p, end.p, st));
+  }
+  raw.release();
+  DArr<uint32_t> cnt;
+  DArr<int> bad;
+  HM_TRY(cnt.alloc(ctx, n_edges));
+  HM_TRY(bad.alloc(ctx, 2));
+  HM_CUDA(cudaMemsetAsync(bad.p, 0, 2 * sizeof(int), st));
+  if (n_edges) {
+    k_row_distinct<<<grid_for((uint64_t)n_edges * 32, kBlock), kBlock, 0, st>>>(raw_off.p, sorted.p, n_edges,
+                                                                              g->n_nodes, cnt.p, bad.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(g->h2v_off.alloc(ctx, (size_t)n_edges + 1));
+  HM_TRY(exclusive_scan(ctx, cnt.p, g->h2v_off.p, n_edges));
+  uint64_t total = 0;
+  HM_CUDA(cudaMemcpyAsync(&total, g->h2v_off.p + n_edges, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_TRY(g->esize.alloc(ctx, n_edges));
+  if (n_edges) {
+    k_u32_to_u8_checked<<<grid_for(n_edges, kBlock), kBlock, 0, st>>>(cnt.p, n_edges, g->esize.p, HM_MAX_EDGE_SIZE,
+                                                                      bad.p + 1);
+    HM_LAUNCH_CHECK();
+  }
+  int hbad[2] = {0, 0};
+  HM_CUDA(cudaMemcpyAsync(hbad, bad.p, sizeof(hbad), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  if (hbad[0]) return set_error(HM_ERR_INVALID, "hm_graph_build: a member id is >= n_nodes (%u)", g->n_nodes);
+  if (hbad[1]) return set_error(HM_ERR_LIMIT, "hm_graph_build: a hyperedge has more than %d distinct members", HM_MAX_EDGE_SIZE);
+  HM_TRY(g->h2v_mem.alloc(ctx, total));
+  if (n_edges) {
+    k_row_distinct_write<<<grid_for((uint64_t)n_edges * 32, kBlock), kBlock, 0, st>>>(raw_off.p, sorted.p, n_edges,
+                                                                                    g->h2v_off.p, g->h2v_mem.p);
+    HM_LAUNCH_CHECK();
+  }
+  g->h2v_len = static_cast<DArr<uint32_t>&&>(cnt);
+  g->h2v_tail = total;
+  g->n_slots = n_edges;
+  g->n_live = n_edges;
+  const uint32_t words = (n_edges + 31) / 32;
+  HM_TRY(g->live_bits.alloc(ctx, words ? words : 1));
+  k_fill_live_bits<<<grid_for(words ? words : 1, kBlock), kBlock, 0, st>>>(g->live_bits.p, words, n_edges);
+  HM_LAUNCH_CHECK();
+  return HM_OK;
+}
+
+int build_v2h(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint64_t nnz = g->h2v_tail;
+  const uint32_t V = g->n_nodes;
+  DArr<uint32_t> keys, vals, keys_out;
+  HM_TRY(keys.alloc(ctx, nnz));
+  HM_TRY(vals.alloc(ctx, nnz));
+  HM_TRY(keys_out.alloc(ctx, nnz));
+  HM_TRY(g->v2h_edge.alloc(ctx, nnz));
+  HM_TRY(g->v2h_len.alloc(ctx, V));
+  HM_CUDA(cudaMemsetAsync(g->v2h_len.p, 0, sizeof(uint32_t) * V, st));
+  if (g->n_slots) {
+    k_member_pairs<<<grid_for((uint64_t)g->n_slots * 32, kBlock), kBlock, 0, st>>>(
+        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->n_slots, keys.p, vals.p, g->v2h_len.p);
+    HM_LAUNCH_CHECK();
+  }
+  if (nnz) {
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) < V) ++end_bit;
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.p, keys_out.p, vals.p, g->v2h_edge.p, (int64_t)nnz, 0,
+                                            end_bit, st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.p, keys_out.p, vals.p, g->v2h_edge.p, (int64_t)nnz, 0,
+                                            end_bit, st));
+  }
+  HM_TRY(g->v2h_off.alloc(ctx, (size_t)V + 1));
+  HM_TRY(exclusive_scan(ctx, g->v2h_len.p, g->v2h_off.p, V));
+  g->v2h_tail = nnz;
+  return HM_OK;
+}
+
+// H2H rows in chunks of the wedge stream: expand, segmented sort, run-length.
+int build_h2h_rows(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  if (E >= (1u << 24))
+    return set_error(HM_ERR_LIMIT, "H2H build: %u hyperedge slots exceed the 2^24 limit of the packed sort key", E);
+  DArr<uint64_t> wedges, woff;
+  HM_TRY(wedges.alloc(ctx, E));
+  HM_TRY(woff.alloc(ctx, (size_t)E + 1));
+  if (E) {
+    k_wedge_count<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
+                                                                       g->v2h_len.p, E, wedges.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(exclusive_scan(ctx, wedges.p, woff.p, E));
+  std::vector<uint64_t> hw((size_t)E + 1);
+  HM_CUDA(cudaMemcpyAsync(hw.data(), woff.p, sizeof(uint64_t) * ((size_t)E + 1), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  wedges.release();
+  const uint64_t W = hw[E];
+  // The arena is sized by the wedge count, an upper bound on the entries.
+  HM_TRY(g->h2h_off.alloc(ctx, (size_t)E + 1));
+  HM_TRY(g->h2h_len.alloc(ctx, E));
+  HM_TRY(g->h2h_nbr.alloc(ctx, W));
+  HM_TRY(g->h2h_ovl.alloc(ctx, W));
+  HM_TRY(g->h2h_mask.alloc(ctx, W));
+  if (E == 0 || W == 0) {
+    if (E) HM_CUDA(cudaMemsetAsync(g->h2h_len.p, 0, sizeof(uint32_t) * E, st));
+    HM_CUDA(cudaMemsetAsync(g->h2h_off.p, 0, sizeof(uint64_t) * ((size_t)E + 1), st));
+    g->h2h_tail = 0;
+    g->h2h_nnz = 0;
+    return HM_OK;
+  }
+  uint64_t chunk_cap = std::min<uint64_t>(W, 1ull << 28);
+  uint64_t max_row = 0;
+  for (uint32_t r = 0; r < E; ++r) max_row = std::max(max_row, hw[r + 1] - hw[r]);
+  if (max_row >= (1ull << 31)) return set_error(HM_ERR_LIMIT, "H2H build: one row has %llu wedges", (unsigned long long)max_row);
+  chunk_cap = std::max(chunk_cap, max_row);
+  DArr<uint32_t> kin, kout, starts, cnt;
+  DArr<int> beg, end;
+  DArr<uint64_t> loff;
+  HM_TRY(kin.alloc(ctx, chunk_cap));
+  HM_TRY(kout.alloc(ctx, chunk_cap));
+  HM_TRY(starts.alloc(ctx, chunk_cap));
+  // rows per chunk are bounded by E
+  HM_TRY(cnt.alloc(ctx, E));
+  HM_TRY(beg.alloc(ctx, E));
+  HM_TRY(end.alloc(ctx, E));
+  HM_TRY(loff.alloc(ctx, (size_t)E + 1));
+  DArr<uint8_t> sort_tmp;
+  size_t sort_tb = 0;
+  uint64_t out_base = 0;
+  uint32_t r0 = 0;
+  while (r0 < E) {
+    uint32_t r1 = r0;
+    while (r1 < E && hw[r1 + 1] - hw[r0] <= chunk_cap) ++r1;
+    const uint32_t nrows = r1 - r0;
+    const uint64_t base = hw[r0];
+    const uint64_t nk = hw[r1] - base;
+    k_expand<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(
+        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->v2h_off.p, g->v2h_len.p, g->v2h_edge.p, woff.p, base, r0, r1,
+        kin.p);
+    HM_LAUNCH_CHECK();
+    k_chunk_bounds<<<grid_for(nrows, kBlock), kBlock, 0, st>>>(woff.p, base, r0, r1, beg.p, end.p);
+    HM_LAUNCH_CHECK();
+    if (nk) {
+      size_t tb = 0;
+      HM_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, kin.p, kout.p, (int)nk, (int)nrows, beg.p, end.p, st));
+      if (tb > sort_tb) {
+        HM_TRY(sort_tmp.alloc(ctx, tb));
+        sort_tb = tb;
+      }
+      HM_CUDA(cub::DeviceSegmentedSort::SortKeys(sort_tmp.p, tb, kin.p, kout.p, (int)nk, (int)nrows, beg.p, end.p,
+                                                 st));
+    }
+    k_chunk_distinct<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(beg.p, end.p, kout.p, nrows, cnt.p);
+    HM_LAUNCH_CHECK();
+    HM_TRY(exclusive_scan(ctx, cnt.p, loff.p, nrows));
+    k_chunk_starts<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(beg.p, end.p, kout.p, nrows, loff.p,
+                                                                             starts.p);
+    HM_LAUNCH_CHECK();
+    k_chunk_emit<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(
+        beg.p, end.p, kout.p, r0, nrows, loff.p, cnt.p, starts.p, out_base, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
+    HM_LAUNCH_CHECK();
+    uint64_t chunk_total = 0;
+    HM_CUDA(cudaMemcpyAsync(&chunk_total, loff.p + nrows, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    out_base += chunk_total;
+    r0 = r1;
+  }
+  HM_CUDA(cudaMemcpyAsync(g->h2h_off.p + E, &out_base, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  g->h2h_tail = out_base;
+  g->h2h_nnz = out_base;
+  return HM_OK;
+}
+
+int build_plus(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  DArr<uint32_t> cnt;
+  HM_TRY(cnt.alloc(ctx, E));
+  if (E) {
+    k_plus_count<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, E,
+                                                                      cnt.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(g->plus_off.alloc(ctx, (size_t)E + 1));
+  HM_TRY(exclusive_scan(ctx, cnt.p, g->plus_off.p, E));
+  uint64_t total = 0;
+  HM_CUDA(cudaMemcpyAsync(&total, g->plus_off.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  HM_TRY(g->plus_nbr.alloc(ctx, total));
+  HM_TRY(g->plus_os.alloc(ctx, total));
+  HM_TRY(g->plus_mask.alloc(ctx, total));
+  if (E) {
+    k_plus_write<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                      g->h2h_ovl.p, g->h2h_mask.p, g->esize.p, E,
+                                                                      g->plus_off.p, g->plus_nbr.p, g->plus_os.p,
+                                                                      g->plus_mask.p);
+    HM_LAUNCH_CHECK();
+  }
+  g->plus_len = static_cast<DArr<uint32_t>&&>(cnt);
+  g->plus_nnz = total;
+  g->plus_valid = true;
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -1,0 +1,215 @@
+"""Python view of the engine's C ABI (include/hmotif.h).
+
+Mirrors the reference's host interface for this path: a store built once
+from hyperedge lists (constructCBST / CBSTOperations::construct,
+dynamicHyperGraph/include/structure.hpp:38-64), batch insert/delete, query,
+and count calls returning MoCHy's 26 static and THyMe's 96 temporal h-motif
+counts. Every call goes through libhmotif.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import weakref
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr, u32p, u64p, i64p, vp
+
+N_STATIC_CLASSES = 30
+N_STATIC_MOTIFS = 26
+N_TEMPORAL_MOTIFS = 96
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [
+        ("n_slots", C.c_uint32),
+        ("n_live", C.c_uint32),
+        ("n_nodes", C.c_uint32),
+        ("temporal", C.c_int32),
+        ("n_members", C.c_uint64),
+        ("n_adjacent", C.c_uint64),
+        ("n_oriented", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+    ]
+
+
+class Traffic(C.Structure):
+    _fields_ = [
+        ("store_bytes", C.c_uint64),
+        ("merge_bytes", C.c_uint64),
+        ("closed_pair_bytes", C.c_uint64),
+        ("b_static", C.c_uint64),
+        ("probes", C.c_uint64),
+        ("kernel_bytes", C.c_uint64),
+        ("closed_triangles", C.c_uint64),
+    ]
+
+
+class Timings(C.Structure):
+    _fields_ = [
+        ("open_ms", C.c_float),
+        ("closed_ms", C.c_float),
+        ("count_ms", C.c_float),
+        ("update_ms", C.c_float),
+        ("temporal_ms", C.c_float),
+        ("closed_triangles", C.c_uint64),
+    ]
+
+
+_lib.bind(
+    {
+        "hm_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(vp)]),
+        "hm_ctx_destroy": (C.c_int, [vp]),
+        "hm_ctx_memory": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "hm_ctx_stream": (vp, [vp]),
+        "hm_debug_fail_allocations_after": (C.c_int, [C.c_longlong]),
+        "hm_graph_build": (C.c_int, [vp, u64p, u32p, C.c_uint32, C.c_uint32, i64p, C.POINTER(vp)]),
+        "hm_graph_destroy": (C.c_int, [vp]),
+        "hm_graph_info": (C.c_int, [vp, C.POINTER(GraphInfo)]),
+        "hm_graph_query": (C.c_int, [vp, u32p, C.c_uint32, u64p, u32p, C.c_size_t]),
+        "hm_graph_timings": (C.c_int, [vp, C.POINTER(Timings)]),
+        "hm_count_static": (C.c_int, [vp, u64p]),
+        "hm_count_static30": (C.c_int, [vp, u64p]),
+        "hm_count_static30_shard": (C.c_int, [vp, C.c_uint32, C.c_uint32, u64p]),
+        "hm_graph_traffic": (C.c_int, [vp, C.POINTER(Traffic)]),
+        "hm_classify_static": (C.c_int, [C.c_int]),
+        "hm_classify_temporal": (C.c_int, [C.c_int]),
+    }
+)
+
+
+class Context:
+    """One CUDA device, one stream, one device-memory budget."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        h = vp()
+        check(lib.hm_ctx_create(device, mem_budget_bytes, C.byref(h)), "hm_ctx_create")
+        self._h = h
+        self.device = device
+        self._children = weakref.WeakSet()  # graphs are released before the context
+
+    @property
+    def handle(self):
+        return self._h
+
+    def memory(self) -> tuple[int, int]:
+        used, budget = C.c_size_t(), C.c_size_t()
+        check(lib.hm_ctx_memory(self._h, C.byref(used), C.byref(budget)), "hm_ctx_memory")
+        return used.value, budget.value
+
+    def close(self) -> None:
+        if self._h:
+            for child in list(self._children):
+                child.close()
+            lib.hm_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _csr_arrays(offsets, members):
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    mem = np.ascontiguousarray(members, dtype=np.uint32)
+    return off, mem
+
+
+class Graph:
+    """A device-resident hypergraph (H2V, V2H, H2H) owned by a Context."""
+
+    def __init__(self, ctx: Context, offsets, members, n_nodes: int, timestamps=None):
+        off, mem = _csr_arrays(offsets, members)
+        ts = None if timestamps is None else np.ascontiguousarray(timestamps, dtype=np.int64)
+        n_edges = len(off) - 1
+        h = vp()
+        check(
+            lib.hm_graph_build(ctx.handle, ptr(off, C.c_uint64), ptr(mem, C.c_uint32), n_edges, int(n_nodes),
+                               ptr(ts, C.c_int64), C.byref(h)),
+            "hm_graph_build",
+        )
+        self._h = h
+        self.ctx = ctx
+        ctx._children.add(self)
+
+    @classmethod
+    def from_hypergraph(cls, ctx: Context, hg) -> "Graph":
+        return cls(ctx, hg.offsets, hg.members, hg.n_nodes, hg.timestamps)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> GraphInfo:
+        i = GraphInfo()
+        check(lib.hm_graph_info(self._h, C.byref(i)), "hm_graph_info")
+        return i
+
+    def timings(self) -> Timings:
+        t = Timings()
+        check(lib.hm_graph_timings(self._h, C.byref(t)), "hm_graph_timings")
+        return t
+
+    def count_static(self) -> np.ndarray:
+        out = np.zeros(N_STATIC_MOTIFS, np.uint64)
+        check(lib.hm_count_static(self._h, ptr(out, C.c_uint64)), "hm_count_static")
+        return out
+
+    def count_static30(self) -> np.ndarray:
+        out = np.zeros(N_STATIC_CLASSES, np.uint64)
+        check(lib.hm_count_static30(self._h, ptr(out, C.c_uint64)), "hm_count_static30")
+        return out
+
+    def count_static30_shard(self, shard: int, n_shards: int) -> np.ndarray:
+        out = np.zeros(N_STATIC_CLASSES, np.uint64)
+        check(lib.hm_count_static30_shard(self._h, shard, n_shards, ptr(out, C.c_uint64)), "hm_count_static30_shard")
+        return out
+
+    def traffic(self) -> Traffic:
+        t = Traffic()
+        check(lib.hm_graph_traffic(self._h, C.byref(t)), "hm_graph_traffic")
+        return t
+
+    def query(self, ids) -> list[np.ndarray]:
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        n = len(ids)
+        off = np.zeros(n + 1, np.uint64)
+        cap = 256 * max(n, 1)
+        mem = np.zeros(cap, np.uint32)
+        check(lib.hm_graph_query(self._h, ptr(ids, C.c_uint32), n, ptr(off, C.c_uint64), ptr(mem, C.c_uint32), cap),
+              "hm_graph_query")
+        return [mem[off[i] : off[i + 1]].copy() for i in range(n)]
+
+    def close(self) -> None:
+        if self._h:
+            lib.hm_graph_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def classify_static(pattern: int) -> int:
+    return lib.hm_classify_static(pattern)
+
+
+def classify_temporal(pattern: int) -> int:
+    return lib.hm_classify_temporal(pattern)

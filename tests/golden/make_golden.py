@@ -1,0 +1,147 @@
+"""Generates the golden fixtures: outputs of the reference's OWN counters.
+
+Each case is a seeded synthetic input (regenerated by the tests from the
+recorded parameters; its SHA-256 is recorded too) run through the reference
+programs compiled from the reference sources by oracle/build_ref.sh:
+  static   -> MoCHy main_exact and main_exact_par (26 counts)
+  temporal -> THyMe main_thyme and main_thymeP (96 counts)
+The MoCHy sample dataset shipped with the reference (dblp_graph.txt) is
+recorded by its hash and counts only; its test runs where the reference tree
+is present.
+
+    python tests/golden/make_golden.py [--only NAME ...]
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from ipdps26_b200 import gen  # noqa: E402
+from oracle import ref_runner as rr  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+REF_DBLP = Path("/root/reference/MoCHy-master/dblp_graph.txt")
+
+
+def digest(h) -> str:
+    m = hashlib.sha256()
+    m.update(np.ascontiguousarray(h.offsets, np.uint64).tobytes())
+    m.update(np.ascontiguousarray(h.members, np.uint32).tobytes())
+    if h.timestamps is not None:
+        m.update(np.ascontiguousarray(h.timestamps, np.int64).tobytes())
+    return m.hexdigest()
+
+
+# name -> (generator params kwargs of gen.params)
+STATIC_CASES = {}
+for s in range(5):
+    STATIC_CASES[f"tiny-c1-{s}"] = dict(seed=s, n_nodes=60, n_edges=80, k_min=2, k_max=25, size_exp=2.5, pop_exp=1.2,
+                                        pop_offset=0.0)
+for s in range(2):
+    STATIC_CASES[f"c1law-2k-{s}"] = dict(seed=10 + s, n_nodes=1000, n_edges=2000, k_min=2, k_max=25, size_exp=2.5,
+                                         pop_exp=1.2, pop_offset=0.0)
+STATIC_CASES["c2law-3k"] = dict(seed=21, n_nodes=3000, n_edges=3000, k_min=2, k_max=100, size_exp=2.2, pop_exp=1.1,
+                                pop_offset=3.0)
+STATIC_CASES["c2law-10k-flat"] = dict(seed=22, n_nodes=20000, n_edges=10000, k_min=2, k_max=100, size_exp=2.2,
+                                      pop_exp=1.1, pop_offset=1000.0)
+STATIC_CASES["wide-overlaps"] = dict(seed=23, n_nodes=120, n_edges=400, k_min=2, k_max=40, size_exp=1.5, pop_exp=0.8,
+                                     pop_offset=0.0)
+STATIC_CASES["size1-and-dups"] = dict(seed=24, n_nodes=50, n_edges=300, k_min=1, k_max=6, size_exp=1.5, pop_exp=1.0,
+                                      pop_offset=0.0, dedupe=False)
+
+TEMPORAL_CASES = {}
+for s in range(4):
+    TEMPORAL_CASES[f"tiny-c4-{s}"] = dict(
+        gen=dict(seed=s, n_nodes=40, n_edges=60, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2, pop_offset=0.0,
+                 dedupe=False),
+        burst=dict(burst_rate=1e-2, events_per_burst=10, gap_mean=5.0, span=2000), deltas=[50, 300, 5000])
+TEMPORAL_CASES["c4law-20k"] = dict(
+    gen=dict(seed=31, n_nodes=8000, n_edges=20000, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2, pop_offset=0.0,
+             dedupe=False),
+    burst=dict(burst_rate=1e-4, events_per_burst=50, gap_mean=20.0, span=4_000_000), deltas=[1000, 10000, 100000])
+
+
+def static_graph(p):
+    kw = dict(p)
+    dedupe = kw.pop("dedupe", True)
+    return gen.static(gen.params(dedupe=dedupe, **kw))
+
+
+def temporal_graph(c):
+    kw = dict(c["gen"])
+    dedupe = kw.pop("dedupe", False)
+    return gen.temporal(gen.params(dedupe=dedupe, **kw), **c["burst"])
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*")
+    ap.add_argument("--timeout", type=float, default=900)
+    a = ap.parse_args()
+    sp = OUT / "static_golden.json"
+    tp = OUT / "temporal_golden.json"
+    sg = json.loads(sp.read_text()) if sp.exists() else {}
+    tg = json.loads(tp.read_text()) if tp.exists() else {}
+    want = set(a.only) if a.only else None
+
+    if REF_DBLP.exists() and (want is None or "dblp" in want):
+        lines = REF_DBLP.read_text().splitlines()
+        off, mem = [0], []
+        for ln in lines:
+            row = []
+            for t in ln.split(","):
+                v = int(t)
+                if v not in row:
+                    row.append(v)
+            mem += row
+            off.append(len(mem))
+        off, mem = np.array(off, np.uint64), np.array(mem, np.uint32)
+        c, w, _ = rr.run_mochy(off, mem, threads=None, timeout=a.timeout)
+        cp, wp, _ = rr.run_mochy(off, mem, threads=8, timeout=a.timeout)
+        assert np.array_equal(c, cp)
+        sg["dblp"] = dict(file_sha256=hashlib.sha256(REF_DBLP.read_bytes()).hexdigest(), counts26=c.tolist(),
+                          n_edges=len(off) - 1, source="MoCHy-master/dblp_graph.txt", mochy_wall_s=round(w, 3))
+        print("dblp", w)
+
+    for name, p in STATIC_CASES.items():
+        if want is not None and name not in want:
+            continue
+        h = static_graph(p)
+        t0 = time.time()
+        c, w, _ = rr.run_mochy(h.offsets, h.members, threads=None, timeout=a.timeout)
+        cp, wp, _ = rr.run_mochy(h.offsets, h.members, threads=8, timeout=a.timeout)
+        assert np.array_equal(c, cp), name
+        sg[name] = dict(params=p, sha256=digest(h), n_edges=h.n_edges, n_members=int(len(h.members)),
+                        counts26=c.tolist(), mochy_wall_s=round(w, 3), mochy_par8_wall_s=round(wp, 3))
+        print(name, h.n_edges, round(time.time() - t0, 2), "s")
+        sp.write_text(json.dumps(sg, indent=1))
+
+    for name, c in TEMPORAL_CASES.items():
+        if want is not None and name not in want:
+            continue
+        h = temporal_graph(c)
+        rec = dict(params=c, sha256=digest(h), n_events=h.n_edges, counts96={})
+        for d in c["deltas"]:
+            t0 = time.time()
+            x, w, _ = rr.run_thyme(h.offsets, h.members, h.timestamps, d, threads=None, timeout=a.timeout)
+            y, wp, _ = rr.run_thyme(h.offsets, h.members, h.timestamps, d, threads=8, timeout=a.timeout)
+            assert np.array_equal(x, y), (name, d)
+            rec["counts96"][str(d)] = x.tolist()
+            print(name, d, round(time.time() - t0, 2), "s")
+        tg[name] = rec
+        tp.write_text(json.dumps(tg, indent=1))
+    sp.write_text(json.dumps(sg, indent=1))
+    tp.write_text(json.dumps(tg, indent=1))
+
+
+if __name__ == "__main__":
+    main()

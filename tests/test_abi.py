@@ -1,0 +1,53 @@
+"""The C ABI library loads and exports every entry point include/*.h declares."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(hm_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ["hm_ctx_create", "hm_graph_build", "hm_count_static", "hm_graph_query"]:
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from ipdps26_b200 import _lib
+
+    missing = [n for n in declared_functions() if not hasattr(_lib.lib, n)]
+    assert not missing, f"symbols declared in include/*.h but not exported: {missing}"
+
+
+def test_status_strings():
+    from ipdps26_b200._lib import lib
+
+    assert lib.hm_status_string(0) == b"ok"
+    assert b"invalid" in lib.hm_status_string(-1)
+
+
+def test_no_device_means_clean_error():
+    """Without a GPU, creating a context fails with a status, never exits."""
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HmError
+
+    try:
+        engine.Context(0)
+    except HmError as e:
+        assert e.status < 0
+    else:
+        raise AssertionError("context creation succeeded without a device")

@@ -1,0 +1,89 @@
+"""The CPU oracle (C restatement of MoCHy / THyMe exact) against the
+reference programs' own outputs (golden fixtures) and against brute force."""
+import hashlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.helpers import csr, digest, load_golden, random_graph, static_case, temporal_case
+
+REF_DBLP = Path("/root/reference/MoCHy-master/dblp_graph.txt")
+
+
+@pytest.mark.parametrize("name", sorted(load_golden("static")))
+def test_static_oracle_matches_mochy(name):
+    rec = load_golden("static")[name]
+    if name == "dblp":
+        if not REF_DBLP.exists():
+            pytest.skip("reference dataset not present")
+        assert hashlib.sha256(REF_DBLP.read_bytes()).hexdigest() == rec["file_sha256"]
+        rows = []
+        for ln in REF_DBLP.read_text().splitlines():
+            r = []
+            for t in ln.split(","):
+                if int(t) not in r:
+                    r.append(int(t))
+            rows.append(r)
+        off, mem = csr(rows)
+        n_nodes = int(mem.max()) + 1
+    else:
+        if rec["n_edges"] > 3000:
+            pytest.skip("large case: covered by the GPU parity test")
+        h = static_case(rec["params"])
+        assert digest(h) == rec["sha256"], "generator output changed"
+        off, mem, n_nodes = h.offsets, h.members, h.n_nodes
+    got = oracle.to26(oracle.static30(off, mem, n_nodes))
+    assert got.tolist() == rec["counts26"]
+
+
+@pytest.mark.parametrize("name", sorted(load_golden("temporal")))
+def test_temporal_oracle_matches_thyme(name):
+    rec = load_golden("temporal")[name]
+    if rec["n_events"] > 2000:
+        pytest.skip("large case: covered by the GPU parity test")
+    h = temporal_case(rec["params"])
+    assert digest(h) == rec["sha256"], "generator output changed"
+    for d, want in rec["counts96"].items():
+        got = oracle.temporal96(h.offsets, h.members, h.timestamps, int(d))
+        assert got.tolist() == want, d
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_static_oracle_matches_brute_force(seed):
+    rng = np.random.default_rng(seed)
+    off, mem = random_graph(rng, 45, 30, 7, p_repeat=0.3)
+    n_nodes = 30
+    a = oracle.static30(off, mem, n_nodes)
+    b = oracle.static30_brute(off, mem)
+    assert a.tolist() == b.tolist()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_temporal_oracle_matches_brute_force(seed):
+    rng = np.random.default_rng(100 + seed)
+    off, mem = random_graph(rng, 40, 12, 4)
+    # repeat some node-sets (THyMe's motifs 87-96)
+    rows = [mem[off[i]:off[i + 1]].tolist() for i in range(len(off) - 1)]
+    for i in range(0, len(rows), 5):
+        rows[i] = rows[max(0, i - 3)]
+    off, mem = csr(rows)
+    times = np.cumsum(rng.integers(1, 20, size=len(rows))).astype(np.int64)
+    for delta in (15, 60, 400):
+        a = oracle.temporal96(off, mem, times, delta)
+        b = oracle.temporal96_brute(off, mem, times, delta)
+        assert a.tolist() == b.tolist()
+        assert a[86:].sum() > 0 or delta == 15
+
+
+def test_class_rules_agree_with_oracle():
+    from ipdps26_b200 import engine
+
+    L = oracle.lib()
+    for p in range(128):
+        assert engine.classify_static(p) == L.hmo_static_class_bits(p)
+        assert engine.classify_temporal(p) == L.hmo_temporal_class_bits(p)
+    # 30 static classes and 96 temporal motifs are each hit by some pattern
+    assert {engine.classify_static(p) for p in range(128)} - {-1} == set(range(30))
+    assert {engine.classify_temporal(p) for p in range(128)} - {-1} == set(range(96))

@@ -1,0 +1,121 @@
+"""Static 26/30-class counts on the GPU, through the C ABI, against the
+reference's outputs (golden fixtures) and the CPU oracle."""
+from math import comb
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.helpers import csr, digest, load_golden, random_graph, static_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(k for k in load_golden("static") if k != "dblp"))
+def test_static_matches_mochy_golden(ctx, name):
+    from ipdps26_b200 import engine
+
+    rec = load_golden("static")[name]
+    h = static_case(rec["params"])
+    assert digest(h) == rec["sha256"]
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        assert g.count_static().tolist() == rec["counts26"]
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_static_matches_oracle_random(ctx, seed):
+    from ipdps26_b200 import engine
+
+    rng = np.random.default_rng(seed)
+    n_nodes = int(rng.integers(5, 80))
+    off, mem = random_graph(rng, int(rng.integers(1, 300)), n_nodes, int(rng.integers(1, 12)), p_repeat=0.2)
+    want = oracle.static30(off, mem, n_nodes)
+    with engine.Graph(ctx, off, mem, n_nodes) as g:
+        assert g.count_static30().tolist() == want.tolist()
+
+
+def test_static_repeated_hyperedges(ctx):
+    """Repeated hyperedges feed the four classes MoCHy does not report."""
+    from ipdps26_b200 import engine
+
+    rows = [[0, 1], [0, 1], [1, 2], [0, 1, 2], [0, 1, 2], [2, 3], [3], [3]]
+    off, mem = csr(rows)
+    want = oracle.static30(off, mem, 4)
+    assert any(want[k] for k in (0, 1, 4, 6))
+    with engine.Graph(ctx, off, mem, 4) as g:
+        assert g.count_static30().tolist() == want.tolist()
+
+
+@pytest.mark.parametrize("rows,n_nodes", [([], 1), ([[0]], 1), ([[0, 1]], 2), ([[0, 1], [2, 3]], 4),
+                                         ([[0, 1], [1, 2]], 3)])
+def test_static_tiny_edge_cases(ctx, rows, n_nodes):
+    from ipdps26_b200 import engine
+
+    off, mem = csr(rows)
+    want = oracle.static30(off, mem, n_nodes)
+    with engine.Graph(ctx, off, mem, n_nodes) as g:
+        assert g.count_static30().tolist() == want.tolist()
+
+
+@pytest.mark.parametrize("n", [300, 5000])
+def test_static_star_clique(ctx, n):
+    """n hyperedges {0, i}: every triple is closed with g = 1 (class 3).
+    n = 5000 gives oriented rows longer than the shared-memory hash table."""
+    from ipdps26_b200 import engine
+
+    rows = [[0, i + 1] for i in range(n)]
+    off, mem = csr(rows)
+    with engine.Graph(ctx, off, mem, n + 1) as g:
+        got = g.count_static30()
+    want = np.zeros(30, np.uint64)
+    want[3] = comb(n, 3)
+    assert got.tolist() == want.tolist()
+
+
+def test_static_c1law_against_oracle(ctx):
+    from ipdps26_b200 import engine, gen
+
+    h = gen.static(gen.config1(seed=77, n_nodes=600, n_edges=1200))
+    want = oracle.static30(h.offsets, h.members, h.n_nodes)
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        assert g.count_static30().tolist() == want.tolist()
+        assert g.count_static30().tolist() == want.tolist()  # repeatable
+
+
+def test_query_returns_sorted_members(ctx):
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HmError
+
+    rows = [[5, 3, 3, 1], [2], [4, 0, 2]]
+    off, mem = csr(rows)
+    with engine.Graph(ctx, off, mem, 6) as g:
+        q = g.query([2, 0, 1])
+        assert [x.tolist() for x in q] == [[0, 2, 4], [1, 3, 5], [2]]
+        with pytest.raises(HmError) as e:
+            g.query([3])
+        assert e.value.status == -5
+
+
+def test_build_rejects_bad_input(ctx):
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HmError
+
+    off, mem = csr([[0, 1], [1, 9]])
+    with pytest.raises(HmError) as e:
+        engine.Graph(ctx, off, mem, 5)
+    assert e.value.status == -1
+    off, mem = csr([list(range(300))])
+    with pytest.raises(HmError) as e:
+        engine.Graph(ctx, off, mem, 300)
+    assert e.value.status == -8
+
+
+@pytest.mark.parametrize("n_shards", [2, 3, 8])
+def test_static_shards_sum_to_full_count(ctx, n_shards):
+    from ipdps26_b200 import engine, gen
+
+    h = gen.static(gen.config2(seed=9, n_nodes=3000, n_edges=6000, q=3.0))
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        full = g.count_static30()
+        parts = sum(g.count_static30_shard(s, n_shards) for s in range(n_shards))
+    assert parts.tolist() == full.tolist()
