@@ -137,6 +137,7 @@ struct hm_graph {
   bool work_valid = false;
   hm::DArr<uint32_t> work;  // centres owning oriented wedges, heaviest first
   uint32_t n_work = 0;
+  uint32_t n_work_big = 0;  // the first n_work_big centres have rows longer than the small-table limit
   hm::DArr<unsigned long long> counters;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool ev_ready = false;

@@ -38,9 +38,11 @@ constexpr unsigned kOpenBlock = 256;
 constexpr unsigned kOpenWarps = kOpenBlock / kWarp;
 constexpr unsigned kClosedBlock = 256;
 constexpr unsigned kClosedWarps = kClosedBlock / kWarp;
+constexpr unsigned kUnroll = 4;               // probes in flight per lane
 constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair classes
-constexpr unsigned kHashSlotsMax = 8192;     // shared-memory hash table capacity
-constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
+// Two launch shapes of the closed phase: rows up to kSmallRow with a 4096-slot
+// table (4 blocks per SM), longer rows with an 8192-slot table (2 per SM).
+constexpr unsigned kSmallRow = 1024;
 constexpr uint32_t kEmpty = 0xffffffffu;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -197,7 +199,9 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
 // triangles (all three overlaps 1, the same shared node) are only counted
 // per size category in registers; the others are classified and their four
 // counter updates aggregated across the lanes that share them.
-__global__ void __launch_bounds__(kClosedBlock, 2) k_closed(ClosedArgs A) {
+template <unsigned kHashSlotsMax, unsigned kMinBlocks>
+__global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
+  constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
   extern __shared__ uint64_t smem64[];
   uint64_t* smask = smem64;                                            // kHashSlotsMax
   uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kHashSlotsMax); // kHashSlotsMax
@@ -246,75 +250,93 @@ __global__ void __launch_bounds__(kClosedBlock, 2) k_closed(ClosedArgs A) {
       const uint64_t bo = A.poff[b];
       const uint32_t bd = A.plen[b];
       uint32_t star0 = 0, star1 = 0, star2 = 0;
-      for (uint32_t j = lane; j < bd; j += kWarp) {
-        const uint32_t c = A.pnbr[bo + j];
-        uint32_t cac = 0;
-        uint64_t mac = 0;
-        if (in_smem) {
-          uint32_t h = hash_slot(c, shift);
-          uint32_t k = keys[h];
-          while (k != c && k != kEmpty) {
-            h = (h + 1) & mask;
-            k = keys[h];
-          }
-          if (k == c) {
-            cac = sovl[h];
-            mac = smask[h];
-            if (flags) {
-              A.edge_flags[ao + mac] = 1;
-              A.edge_flags[ao + bi] = 1;
-              A.edge_flags[bo + j] = 1;
-              mac = A.pmask[ao + mac];
-            }
-          }
-        } else {
-          uint32_t lo = 0, hi = ad;
-          const uint32_t* row = A.pnbr + ao;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (row[mid] < c) lo = mid + 1;
-            else hi = mid;
-          }
-          if (lo < ad && row[lo] == c) {
-            cac = A.pos[ao + lo] & 0xffu;
-            mac = A.pmask[ao + lo];
-            if (flags) {
-              A.edge_flags[ao + lo] = 1;
-              A.edge_flags[ao + bi] = 1;
-              A.edge_flags[bo + j] = 1;
-            }
+      // kUnroll probes per lane per round: their id and overlap/size loads are
+      // issued together so several global loads are in flight per lane.
+      for (uint32_t j0 = 0; j0 < bd; j0 += kWarp * kUnroll) {
+        uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+        for (unsigned u = 0; u < kUnroll; ++u) {
+          const uint32_t j = j0 + u * kWarp + lane;
+          cv[u] = kEmpty;
+          ov[u] = 0;
+          if (j < bd) {
+            cv[u] = __ldg(A.pnbr + bo + j);
+            ov[u] = __ldg(A.pos + bo + j);
           }
         }
-        if (!cac) continue;
-        const uint32_t osc = A.pos[bo + j];
-        const uint32_t cbc = osc & 0xffu, sc = osc >> 8;
-        uint32_t g;
-        if (exact_masks) {
-          if ((cab | cac | cbc) == 1 && mab == mac) {
-            const uint32_t cc = size_cat(sc);
-            star0 += cc == 0;
-            star1 += cc == 1;
-            star2 += cc == 2;
-            continue;
+#pragma unroll
+        for (unsigned u = 0; u < kUnroll; ++u) {
+          const uint32_t c = cv[u];
+          if (c == kEmpty) continue;
+          uint32_t cac = 0;
+          uint64_t mac = 0;
+          if (in_smem) {
+            uint32_t h = hash_slot(c, shift);
+            uint32_t k = keys[h];
+            while (k != c && k != kEmpty) {
+              h = (h + 1) & mask;
+              k = keys[h];
+            }
+            if (k == c) {
+              cac = sovl[h];
+              mac = smask[h];
+              if (flags) {
+                const uint32_t j = j0 + u * kWarp + lane;
+                A.edge_flags[ao + mac] = 1;
+                A.edge_flags[ao + bi] = 1;
+                A.edge_flags[bo + j] = 1;
+                mac = A.pmask[ao + mac];
+              }
+            }
+          } else {
+            uint32_t lo = 0, hi = ad;
+            const uint32_t* row = A.pnbr + ao;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (row[mid] < c) lo = mid + 1;
+              else hi = mid;
+            }
+            if (lo < ad && row[lo] == c) {
+              cac = A.pos[ao + lo] & 0xffu;
+              mac = A.pmask[ao + lo];
+              if (flags) {
+                const uint32_t j = j0 + u * kWarp + lane;
+                A.edge_flags[ao + lo] = 1;
+                A.edge_flags[ao + bi] = 1;
+                A.edge_flags[bo + j] = 1;
+              }
+            }
           }
-          g = __popcll(mab & mac);
-        } else {
-          g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
-        }
-        const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
-        if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-        // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
-        const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
-        const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
-        const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
-        const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
-        const unsigned peers = __match_any_sync(__activemask(), key);
-        if (lane == (unsigned)(__ffs(peers) - 1)) {
-          const unsigned long long n = (unsigned long long)__popc(peers);
-          atomicAdd(&wc[k], n);
-          atomicAdd(&wc[30 + oa], n);
-          atomicAdd(&wc[30 + ob], n);
-          atomicAdd(&wc[30 + oc], n);
+          if (!cac) continue;
+          const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
+          uint32_t g;
+          if (exact_masks) {
+            if ((cab | cac | cbc) == 1 && mab == mac) {
+              const uint32_t cc = size_cat(sc);
+              star0 += cc == 0;
+              star1 += cc == 1;
+              star2 += cc == 2;
+              continue;
+            }
+            g = __popcll(mab & mac);
+          } else {
+            g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
+          }
+          const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
+          if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+          // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
+          const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
+          const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
+          const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
+          const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
+          const unsigned peers = __match_any_sync(__activemask(), key);
+          if (lane == (unsigned)(__ffs(peers) - 1)) {
+            const unsigned long long n = (unsigned long long)__popc(peers);
+            atomicAdd(&wc[k], n);
+            atomicAdd(&wc[30 + oa], n);
+            atomicAdd(&wc[30 + ob], n);
+            atomicAdd(&wc[30 + oc], n);
+          }
         }
       }
       if (cab == 1 && exact_masks) {
@@ -340,7 +362,9 @@ __global__ void __launch_bounds__(kClosedBlock, 2) k_closed(ClosedArgs A) {
 }
 
 // Work estimate per centre: sum of d+(b) over b in N+(a); centres with fewer
-// than two oriented neighbours own no triangle and are dropped.
+// than two oriented neighbours own no triangle and are dropped (key 0). Rows
+// longer than kSmallRow get the top bit so they sort first and go to the
+// large-table launch.
 __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, uint32_t n,
                               uint64_t* est, uint32_t* ids) {
   for (uint64_t a = global_warp(); a < n; a += n_warps()) {
@@ -350,7 +374,9 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
       for (uint32_t i = lane_id(); i < d; i += kWarp) s += plen[pnbr[poff[a] + i]];
     s = warp_sum(s);
     if (lane_id() == 0) {
-      est[a] = (d >= 2 && s > 0) ? s + d : 0;
+      uint64_t key = (d >= 2 && s > 0) ? s + d : 0;
+      if (key && d > kSmallRow) key |= 1ull << 63;
+      est[a] = key;
       ids[a] = (uint32_t)a;
     }
   }
@@ -358,7 +384,8 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
 
 }  // namespace
 
-size_t closed_smem_bytes() { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * kHashSlotsMax; }
+constexpr size_t closed_smem_bytes(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * slots; }
+constexpr unsigned kBigSlots = 8192, kSmallSlots = 4096;
 
 // Centres that own at least one oriented wedge, heaviest first.
 static int closed_worklist(hm_graph* g) {
@@ -392,6 +419,14 @@ static int closed_worklist(hm_graph* g) {
     else hi = mid;
   }
   g->n_work = lo;
+  lo = 0;
+  hi = g->n_work;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (h[mid] >> 63) lo = mid + 1;
+    else hi = mid;
+  }
+  g->n_work_big = lo;
   g->work_valid = true;
   return HM_OK;
 }
@@ -411,7 +446,10 @@ int prepare_static(hm_graph* g) {
   }
   static bool attr_set = false;
   if (!attr_set) {
-    HM_CUDA(cudaFuncSetAttribute(k_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)closed_smem_bytes()));
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kBigSlots)));
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kSmallSlots)));
     attr_set = true;
   }
   return HM_OK;
@@ -419,13 +457,13 @@ int prepare_static(hm_graph* g) {
 
 // Launches both phases for one shard of the centres; the counters land in
 // g->counters ([0,30) closed classes, [30,36) open-pair removals, [36,42)
-// open-pair counts, [42] work queue). edge_flags is for diagnostics.
+// open-pair counts, [42..43] work queues). edge_flags is for diagnostics.
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
-  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 43, st));
+  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 44, st));
   HM_CUDA(cudaEventRecord(g->ev[0], st));
   if (E) {
     k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
@@ -434,13 +472,23 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
     HM_LAUNCH_CHECK();
   }
   HM_CUDA(cudaEventRecord(g->ev[1], st));
-  if (g->n_work > shard) {
+  // rows longer than kSmallRow first (8192-slot tables, 2 blocks per SM),
+  // then the rest (4096-slot tables, 4 blocks per SM)
+  for (int part = 0; part < 2; ++part) {
+    const uint32_t begin = part ? g->n_work_big : 0, end = part ? g->n_work : g->n_work_big;
+    const uint32_t n = end - begin;
+    if (n <= shard) continue;
     ClosedArgs A{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p,
-                 g->esize.p, g->work.p, g->n_work, shard, n_shards, reinterpret_cast<unsigned int*>(dev + 42), dev,
-                 edge_flags};
-    const uint32_t items = (g->n_work - shard + n_shards - 1) / n_shards;
-    const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
-    k_closed<<<grid, kClosedBlock, closed_smem_bytes(), st>>>(A);
+                 g->esize.p, g->work.p + begin, n, shard, n_shards,
+                 reinterpret_cast<unsigned int*>(dev + 42 + part), dev, edge_flags};
+    const uint32_t items = (n - shard + n_shards - 1) / n_shards;
+    if (part == 0) {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
+      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
+    } else {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, items);
+      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
+    }
     HM_LAUNCH_CHECK();
   }
   HM_CUDA(cudaEventRecord(g->ev[2], st));
@@ -448,7 +496,7 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
 }
 
 int finish_static(hm_graph* g, uint64_t out30[30]) {
-  unsigned long long h[43];
+  unsigned long long h[44];
   cudaStream_t st = g->ctx->stream;
   HM_CUDA(cudaMemcpyAsync(h, g->counters.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
