@@ -155,7 +155,35 @@ int hm_graph_info(const hm_graph* g, hm_graph_info_t* info);
 int hm_graph_query(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t* offsets_out, uint32_t* members_out,
                    size_t members_cap);
 
+/* One update batch: delete the live hyperedges del_ids[0..n_del) (each at
+ * most once), then insert n_ins hyperedges given as a CSR (ins_offsets has
+ * n_ins + 1 entries starting at 0; members as in hm_graph_build). Inserted
+ * hyperedges take the smallest free ids first, ascending (ids freed by this
+ * batch included), then new ids after the largest; the ids are written to
+ * assigned_ids_out (n_ins entries, may be NULL). If delta30_out is not NULL it
+ * receives the exact change of the 30 static classes (new minus old), counted
+ * on the device from the triples the batch touches only.
+ * Replaces deleteCBST / unfillCBST / insertCBST / fillCBST
+ * (dynamicHyperGraph/structure/operations.cu:82-356, 439-453) on H2V, V2H and
+ * H2H together, the host rebuild of the updated graph
+ * (dynamicHyperGraph/src/main.cu:333-342), and computeMotifCountsDelta
+ * (dynamicHyperGraph/include/motif_update.hpp:13-19,
+ * src/HMotifCountUpdate.cu:228-301), whose result is not exact in general.
+ * Temporal graphs are immutable (HM_ERR_STATE). */
+int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32_t n_del, const uint64_t* ins_offsets,
+                         const uint32_t* ins_members, uint32_t n_ins, uint32_t* assigned_ids_out,
+                         int64_t* delta30_out);
+/* The ids of the live hyperedges in ascending order; *n_out receives their
+ * number (out may be NULL to query it). */
+int hm_graph_live_ids(const hm_graph* g, uint32_t* out, uint32_t cap, uint32_t* n_out);
+
 /* ---- counts ------------------------------------------------------------ */
+/* 30-class counts of the connected triples that contain at least one of the
+ * live hyperedges ids[0..n) (repeats ignored). The exact recount of a batch
+ * is this count for the inserted ids after it minus this count for the
+ * deleted ids before it. */
+int hm_count_touching30(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t out30[HM_N_STATIC_CLASSES]);
+
 /* MoCHy's 26 static h-motif counts over all connected hyperedge triples.
  * Replaces computeMotifCounts (dynamicHyperGraph/include/motif.hpp:10-13,
  * src/HMotifCount.cu:97-125), which returns nothing and counts closed

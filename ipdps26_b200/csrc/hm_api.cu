@@ -1,6 +1,8 @@
 // C ABI entry points for graphs: build, destroy, info, query, static counts.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "hm_classes.h"
 #include "hm_device.h"
@@ -13,12 +15,9 @@ __global__ void k_query_sizes(const uint32_t* ids, uint32_t n, uint32_t n_slots,
                               const uint32_t* h2v_len, uint32_t* sizes, int* bad) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t id = ids[i];
-    if (id >= n_slots || !((live_bits[id >> 5] >> (id & 31)) & 1u)) {
-      atomicExch(bad, 1);
-      sizes[i] = 0;
-    } else {
-      sizes[i] = h2v_len[id];
-    }
+    const bool live = id < n_slots && ((live_bits[id >> 5] >> (id & 31)) & 1u);
+    if (!live) atomicExch(bad, 1);
+    if (sizes) sizes[i] = live ? h2v_len[id] : 0;
   }
 }
 
@@ -93,7 +92,7 @@ extern "C" int hm_graph_info(const hm_graph* g, hm_graph_info_t* info) {
   info->n_slots = g->n_slots;
   info->n_live = g->n_live;
   info->n_nodes = g->n_nodes;
-  info->n_members = g->h2v_tail;
+  info->n_members = g->h2v_nnz;
   info->n_adjacent = g->h2h_nnz;
   info->n_oriented = g->plus_valid ? g->plus_nnz : 0;
   info->device_bytes = g->ctx->used.load();
@@ -183,4 +182,66 @@ extern "C" int hm_classify_temporal(int pattern) {
   for (int m = 0; m < HM_N_TEMPORAL_MOTIFS; ++m)
     if (hm::kTemporalMotifPattern[m] == (pattern & 127)) return m;
   return -1;
+}
+
+namespace hm {
+int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
+                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
+int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]);
+}  // namespace hm
+
+extern "C" int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32_t n_del,
+                                    const uint64_t* ins_offsets, const uint32_t* ins_members, uint32_t n_ins,
+                                    uint32_t* assigned_ids_out, int64_t* delta30_out) {
+  if (!g || (n_del && !del_ids) || (n_ins && (!ins_offsets || (ins_offsets[n_ins] && !ins_members))))
+    return hm::set_error(HM_ERR_INVALID, "hm_graph_apply_batch: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::apply_batch(g, del_ids, n_del, ins_offsets, ins_members, n_ins, assigned_ids_out, delta30_out);
+}
+
+extern "C" int hm_count_touching30(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t out30[HM_N_STATIC_CLASSES]) {
+  if (!g || !out30 || (n && !ids)) return hm::set_error(HM_ERR_INVALID, "hm_count_touching30: NULL argument");
+  std::vector<uint32_t> u(ids, ids + n);
+  std::sort(u.begin(), u.end());
+  u.erase(std::unique(u.begin(), u.end()), u.end());
+  CtxLock lock(g->ctx);
+  hm_ctx* ctx = g->ctx;
+  hm::DArr<uint32_t> d;
+  hm::DArr<int> bad;
+  HM_TRY(d.alloc(ctx, u.size()));
+  HM_TRY(bad.alloc(ctx, 1));
+  HM_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+  if (!u.empty()) {
+    HM_CUDA(cudaMemcpyAsync(d.p, u.data(), sizeof(uint32_t) * u.size(), cudaMemcpyHostToDevice, ctx->stream));
+    k_query_sizes<<<hm::grid_for(u.size(), kBlock), kBlock, 0, ctx->stream>>>(d.p, (uint32_t)u.size(), g->n_slots,
+                                                                              g->live_bits.p, g->h2v_len.p, nullptr,
+                                                                              bad.p);
+    HM_LAUNCH_CHECK();
+  }
+  int hbad = 0;
+  HM_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  HM_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (hbad) return hm::set_error(HM_ERR_NOT_LIVE, "hm_count_touching30: an id is not a live hyperedge");
+  return hm::count_touching(g, d.p, (uint32_t)u.size(), out30);
+}
+
+extern "C" int hm_graph_live_ids(const hm_graph* g, uint32_t* out, uint32_t cap, uint32_t* n_out) {
+  if (!g || !n_out) return hm::set_error(HM_ERR_INVALID, "hm_graph_live_ids: NULL argument");
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  cudaSetDevice(g->ctx->device);
+  const uint32_t words = (g->n_slots + 31) / 32;
+  std::vector<uint32_t> bits(words);
+  if (words)
+    HM_CUDA(cudaMemcpyAsync(bits.data(), g->live_bits.p, sizeof(uint32_t) * words, cudaMemcpyDeviceToHost,
+                            g->ctx->stream));
+  HM_CUDA(cudaStreamSynchronize(g->ctx->stream));
+  uint32_t n = 0;
+  for (uint32_t id = 0; id < g->n_slots; ++id)
+    if ((bits[id >> 5] >> (id & 31)) & 1u) {
+      if (out && n < cap) out[n] = id;
+      ++n;
+    }
+  *n_out = n;
+  if (out && n > cap) return hm::set_error(HM_ERR_CAPACITY, "hm_graph_live_ids: %u live ids > capacity %u", n, cap);
+  return HM_OK;
 }

@@ -1,0 +1,296 @@
+// Counts of the connected triples that touch a set of marked hyperedges (all
+// 30 static classes). The exact incremental recount of a batch is this count
+// for the inserted ids on the new graph minus it for the deleted ids on the
+// old graph.
+//
+// Same open/closed split as the static count (hm_static.cu):
+//   * open phase over the centres that are marked or adjacent to a marked
+//     hyperedge: pairs {b, c} of the centre's neighbours that contain a marked
+//     hyperedge = all pairs (marked centre) or all pairs minus the pairs of
+//     unmarked neighbours (unmarked centre), counted from histograms;
+//   * closed phase, one block per marked m: row(m) in a shared-memory hash;
+//     each warp takes b in row(m), its lanes walk the neighbours c > b of b
+//     and probe. A triangle {m, b, c} is counted at its smallest marked id.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "hm_classes.h"
+#include "hm_device.h"
+#include "hm_pairs.cuh"
+
+namespace hm {
+namespace {
+
+constexpr unsigned kWarp = 32;
+constexpr unsigned kBlock = 256;
+constexpr unsigned kWarps = kBlock / kWarp;
+constexpr unsigned kSlots = 8192;
+constexpr unsigned kRowMax = kSlots / 2;
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint64_t global_warp() { return ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint64_t n_warps() { return ((uint64_t)gridDim.x * blockDim.x) >> 5; }
+__device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+
+__global__ void k_mark(const uint32_t* ids, uint32_t n, uint8_t* mark) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) mark[ids[i]] = 1;
+}
+
+// flag = marked or adjacent to a marked hyperedge
+__global__ void k_flag_touched(const uint32_t* ids, uint32_t n, const uint64_t* off, const uint32_t* len,
+                               const uint32_t* nbr, uint32_t* flag) {
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t m = ids[i];
+    if (lane_id() == 0) flag[m] = 1;
+    const uint64_t s = off[m];
+    for (uint32_t k = lane_id(); k < len[m]; k += kWarp) flag[nbr[s + k]] = 1;
+  }
+}
+
+__global__ void k_list_flagged(const uint32_t* flag, const uint64_t* pos, uint32_t n, uint32_t* out) {
+  for (uint64_t i = gtid(); i < n; i += gstride())
+    if (flag[i]) out[pos[i]] = (uint32_t)i;
+}
+
+__global__ void __launch_bounds__(kBlock) k_touch_open(const uint32_t* centres, uint32_t n, const uint8_t* mark,
+                                                       const uint64_t* off, const uint32_t* len, const uint32_t* nbr,
+                                                       const uint8_t* ovl, const uint8_t* esize,
+                                                       unsigned long long* out6) {
+  __shared__ uint32_t hist[kWarps][4][256];  // all: type 0/1; unmarked: type 0/1
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  uint64_t acc[6] = {0, 0, 0, 0, 0, 0};
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t a = centres[i];
+    const uint32_t l = len[a];
+    if (l < 2) continue;
+    const uint32_t s = esize[a];
+    const bool ma = mark[a];
+    for (uint32_t k = lane; k <= s; k += kWarp)
+      for (int t = 0; t < 4; ++t) hist[w][t][k] = 0;
+    __syncwarp();
+    const uint64_t base = off[a];
+    for (uint32_t k = lane; k < l; k += kWarp) {
+      const uint32_t b = nbr[base + k];
+      const uint32_t c = ovl[base + k];
+      const uint32_t y = c < esize[b];
+      atomicAdd(&hist[w][y][c], 1u);
+      if (!ma && !mark[b]) atomicAdd(&hist[w][2 + y][c], 1u);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      for (int t = 0; t < 4; ++t)
+        for (uint32_t k = 1; k <= s; ++k) hist[w][t][k] += hist[w][t][k - 1];
+      open_pair_counts(hist[w][0], hist[w][1], s, acc, false);
+      if (!ma) open_pair_counts(hist[w][2], hist[w][3], s, acc, true);
+    }
+    __syncwarp();
+  }
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k)
+      if (acc[k]) atomicAdd(&out6[k], (unsigned long long)acc[k]);
+}
+
+__device__ uint32_t triple_overlap3(const uint64_t* hoff, const uint32_t* hmem, const uint8_t* esize, uint32_t a,
+                                    uint32_t b, uint32_t c) {
+  const uint32_t* x = hmem + hoff[a];
+  const uint32_t* y = hmem + hoff[b];
+  const uint32_t* z = hmem + hoff[c];
+  const uint32_t nx = esize[a], ny = esize[b], nz = esize[c];
+  uint32_t i = 0, j = 0, k = 0, g = 0;
+  while (i < nx && j < ny && k < nz) {
+    const uint32_t u = x[i], v = y[j], t = z[k];
+    const uint32_t m = max(u, max(v, t));
+    if (u == m && v == m && t == m) {
+      ++g; ++i; ++j; ++k;
+    } else {
+      i += (u < m);
+      j += (v < m);
+      k += (t < m);
+    }
+  }
+  return g;
+}
+
+struct TouchArgs {
+  const uint32_t* ids;
+  uint32_t n;
+  const uint8_t* mark;
+  const uint64_t* off;
+  const uint32_t* len;
+  const uint32_t* nbr;
+  const uint8_t* ovl;
+  const uint64_t* mask;
+  const uint64_t* hoff;
+  const uint32_t* hmem;
+  const uint8_t* esize;
+  unsigned int* queue;
+  unsigned long long* out;  // 30 closed classes, 6 open-pair removals
+};
+
+__global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
+  extern __shared__ uint64_t smem64[];
+  uint64_t* smask = smem64;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kSlots);
+  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kSlots);
+  __shared__ unsigned long long wcnt[kWarps][36];
+  __shared__ uint32_t s_item;
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  unsigned long long* wc = wcnt[w];
+  for (unsigned k = lane; k < 36; k += kWarp) wc[k] = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= A.n) break;
+    const uint32_t m = A.ids[item];
+    const uint64_t mo = A.off[m];
+    const uint32_t md = A.len[m];
+    const uint32_t sm = A.esize[m];
+    const bool in_smem = md <= kRowMax;
+    uint32_t shift = 32, hmask = 0;
+    if (in_smem) {
+      uint32_t slots = 64;
+      while (slots < 4 * md && slots < kSlots) slots <<= 1;
+      shift = 32 - (31 - __clz(slots));
+      hmask = slots - 1;
+      for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < md; i += blockDim.x) {
+        const uint32_t key = A.nbr[mo + i];
+        uint32_t h = (key * 2654435761u) >> shift;
+        while (atomicCAS(&keys[h], kEmpty, key) != kEmpty) h = (h + 1) & hmask;
+        smask[h] = A.mask[mo + i];
+        sovl[h] = A.ovl[mo + i];
+      }
+    }
+    __syncthreads();
+    for (uint32_t bi = w; bi < md; bi += kWarps) {
+      const uint32_t b = A.nbr[mo + bi];
+      const uint32_t cmb = A.ovl[mo + bi];
+      const uint64_t mmb = A.mask[mo + bi];
+      const uint32_t sb = A.esize[b];
+      const bool mark_b_before = A.mark[b] && b < m;
+      if (mark_b_before) continue;  // counted at b
+      const uint64_t bo = A.off[b];
+      const uint32_t bl = A.len[b];
+      // first neighbour of b with an id above b
+      uint32_t lo = 0, hi = bl;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A.nbr[bo + mid] <= b) lo = mid + 1;
+        else hi = mid;
+      }
+      for (uint32_t j = lo + lane; j < bl; j += kWarp) {
+        const uint32_t c = A.nbr[bo + j];
+        uint32_t cmc = 0;
+        uint64_t mmc = 0;
+        if (in_smem) {
+          uint32_t h = (c * 2654435761u) >> shift;
+          uint32_t k = keys[h];
+          while (k != c && k != kEmpty) {
+            h = (h + 1) & hmask;
+            k = keys[h];
+          }
+          if (k == c) {
+            cmc = sovl[h];
+            mmc = smask[h];
+          }
+        } else {
+          uint32_t l2 = 0, h2 = md;
+          while (l2 < h2) {
+            const uint32_t mid = (l2 + h2) >> 1;
+            if (A.nbr[mo + mid] < c) l2 = mid + 1;
+            else h2 = mid;
+          }
+          if (l2 < md && A.nbr[mo + l2] == c) {
+            cmc = A.ovl[mo + l2];
+            mmc = A.mask[mo + l2];
+          }
+        }
+        if (!cmc) continue;
+        if (A.mark[c] && c < m) continue;  // counted at c
+        const uint32_t cbc = A.ovl[bo + j];
+        const uint32_t sc = A.esize[c];
+        const uint32_t g = sm <= 64 ? (uint32_t)__popcll(mmb & mmc) : triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
+        const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
+        if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+        const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
+        const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
+        const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
+        const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
+        const unsigned peers = __match_any_sync(__activemask(), key);
+        if (lane == (unsigned)(__ffs(peers) - 1)) {
+          const unsigned long long cnt = (unsigned long long)__popc(peers);
+          atomicAdd(&wc[k], cnt);
+          atomicAdd(&wc[30 + om], cnt);
+          atomicAdd(&wc[30 + ob], cnt);
+          atomicAdd(&wc[30 + oc], cnt);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  __syncwarp();
+  for (unsigned k = lane; k < 36; k += kWarp)
+    if (wc[k]) atomicAdd(&A.out[k], wc[k]);
+}
+
+constexpr size_t touch_smem() { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * kSlots; }
+
+}  // namespace
+
+int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < 30; ++k) out30[k] = 0;
+  if (!n) return HM_OK;
+  const uint32_t E = g->n_slots;
+  DArr<uint8_t> mark;
+  DArr<uint32_t> flag, centres;
+  DArr<uint64_t> pos;
+  DArr<unsigned long long> cnt;
+  HM_TRY(mark.alloc(ctx, E));
+  HM_TRY(flag.alloc(ctx, E));
+  HM_TRY(pos.alloc(ctx, (size_t)E + 1));
+  HM_TRY(cnt.alloc(ctx, 44));
+  HM_CUDA(cudaMemsetAsync(mark.p, 0, E, st));
+  HM_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(uint32_t) * E, st));
+  HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * 44, st));
+  k_mark<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, mark.p);
+  HM_LAUNCH_CHECK();
+  k_flag_touched<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_off.p, g->h2h_len.p,
+                                                                       g->h2h_nbr.p, flag.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(exclusive_scan(ctx, flag.p, pos.p, E));
+  uint64_t nc = 0;
+  HM_CUDA(cudaMemcpyAsync(&nc, pos.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  HM_TRY(centres.alloc(ctx, nc));
+  k_list_flagged<<<grid_for(E, kBlock), kBlock, 0, st>>>(flag.p, pos.p, E, centres.p);
+  HM_LAUNCH_CHECK();
+  k_touch_open<<<grid_for(nc * 32, kBlock), kBlock, 0, st>>>(centres.p, (uint32_t)nc, mark.p, g->h2h_off.p,
+                                                             g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->esize.p,
+                                                             cnt.p + 36);
+  HM_LAUNCH_CHECK();
+  static bool attr = false;
+  if (!attr) {
+    HM_CUDA(cudaFuncSetAttribute(k_touch_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)touch_smem()));
+    attr = true;
+  }
+  TouchArgs A{d_ids, n, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
+              g->h2v_off.p, g->h2v_mem.p, g->esize.p, reinterpret_cast<unsigned int*>(cnt.p + 42), cnt.p};
+  k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n), kBlock, touch_smem(), st>>>(A);
+  HM_LAUNCH_CHECK();
+  unsigned long long h[44];
+  HM_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < 30; ++k) out30[k] = h[k];
+  for (int k = 0; k < 6; ++k) out30[20 + k] += h[36 + k] - h[30 + k];
+  return HM_OK;
+}
+
+}  // namespace hm

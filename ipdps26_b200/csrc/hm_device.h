@@ -6,6 +6,7 @@
 
 #include <atomic>
 #include <cstddef>
+#include <functional>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -110,6 +111,7 @@ struct hm_graph {
   hm::DArr<uint32_t> h2v_len;
   hm::DArr<uint32_t> h2v_mem;
   uint64_t h2v_tail = 0;
+  uint64_t h2v_nnz = 0;  // live members (h2v_tail also counts dead space)
 
   hm::DArr<uint64_t> v2h_off;
   hm::DArr<uint32_t> v2h_len;
@@ -122,7 +124,8 @@ struct hm_graph {
   hm::DArr<uint8_t> h2h_ovl;
   hm::DArr<uint64_t> h2h_mask;
   uint64_t h2h_tail = 0;
-  uint64_t h2h_nnz = 0;
+  uint64_t h2h_nnz = 0;  // live entries
+  uint64_t h2h_cap = 0;  // arena entries allocated
 
   // oriented adjacency (rebuilt lazily after updates)
   bool plus_valid = false;
@@ -160,6 +163,8 @@ namespace hm {
 int build_h2v(hm_graph* g, const uint64_t* h_off, const uint32_t* h_mem, uint32_t n_edges);
 int build_v2h(hm_graph* g);
 int build_h2h_rows(hm_graph* g);
+int h2h_rows_for(hm_graph* g, const uint32_t* d_rows, uint32_t n_rows,
+                 const std::function<int(uint64_t, uint64_t*)>& reserve, uint64_t* written);
 int build_plus(hm_graph* g);
 template <class T>
 int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n);

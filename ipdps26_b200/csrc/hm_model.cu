@@ -117,7 +117,7 @@ extern "C" int hm_graph_traffic(hm_graph* g, hm_traffic_t* t) {
   unsigned long long h[4];
   HM_CUDA(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
-  t->store_bytes = 4ull * g->h2v_tail + 8ull * g->h2h_nnz;
+  t->store_bytes = 4ull * g->h2v_nnz + 8ull * g->h2h_nnz;
   t->merge_bytes = h[0];
   t->closed_pair_bytes = h[1];
   t->b_static = t->store_bytes + t->merge_bytes + t->closed_pair_bytes;

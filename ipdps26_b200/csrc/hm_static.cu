@@ -28,6 +28,7 @@
 
 #include "hm_classes.h"
 #include "hm_device.h"
+#include "hm_pairs.cuh"
 
 namespace hm {
 
@@ -99,29 +100,7 @@ __global__ void __launch_bounds__(kOpenBlock) k_open_pairs(const uint64_t* __res
         h0[k] += h0[k - 1];
         h1[k] += h1[k - 1];
       }
-      const uint64_t n0 = h0[s], n1 = h1[s];
-      // ordered pairs (b, c), b of type t, c of type u, with C_b + C_c <= s - 1
-      uint64_t l00 = 0, l01 = 0, l11 = 0, d0 = 0, d1 = 0;
-      for (uint32_t c1 = 1; c1 + 1 < s; ++c1) {
-        const uint64_t x0 = h0[c1] - h0[c1 - 1], x1 = h1[c1] - h1[c1 - 1];
-        const uint32_t m = s - 1 - c1;
-        l00 += x0 * h0[m];
-        l01 += x0 * h1[m];
-        l11 += x1 * h1[m];
-        if (2 * c1 <= s - 1) {
-          d0 += x0;
-          d1 += x1;
-        }
-      }
-      const uint64_t p00 = (l00 - d0) / 2, p11 = (l11 - d1) / 2, p01 = l01;
-      const uint64_t t00 = n0 * (n0 - (n0 > 0)) / 2, t11 = n1 * (n1 - (n1 > 0)) / 2, t01 = n0 * n1;
-      // open class index = x + 2 * (#ends with an exclusive part)
-      acc[1] += p00;
-      acc[0] += t00 - p00;
-      acc[3] += p01;
-      acc[2] += t01 - p01;
-      acc[5] += p11;
-      acc[4] += t11 - p11;
+      open_pair_counts(h0, h1, s, acc, false);
     }
     __syncwarp();
   }

@@ -13,6 +13,7 @@
 #include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "hm_device.h"
@@ -101,14 +102,14 @@ __global__ void k_fill_live_bits(uint32_t* bits, uint32_t n_words, uint32_t n_li
 // (node, slot) pairs in slot order, so a stable sort by node keeps slots
 // ascending within each node.
 __global__ void k_member_pairs(const uint64_t* off, const uint32_t* len, const uint32_t* mem, uint32_t n,
-                               uint32_t* keys, uint32_t* vals, uint32_t* node_cnt) {
+                               const uint64_t* pair_off, uint32_t* keys, uint32_t* vals, uint32_t* node_cnt) {
   for (uint64_t r = global_warp(); r < n; r += n_warps()) {
-    const uint64_t s = off[r];
+    const uint64_t s = off[r], d = pair_off[r];
     const uint32_t l = len[r];
     for (uint32_t i = lane_id(); i < l; i += kWarp) {
       const uint32_t v = mem[s + i];
-      keys[s + i] = v;
-      vals[s + i] = (uint32_t)r;
+      keys[d + i] = v;
+      vals[d + i] = (uint32_t)r;
       atomicAdd(&node_cnt[v], 1u);
     }
   }
@@ -116,15 +117,20 @@ __global__ void k_member_pairs(const uint64_t* off, const uint32_t* len, const u
 
 // ---- H2H ---------------------------------------------------------------------
 
+// Rows are addressed through an optional list: list position i is slot
+// rows[i] (slot i when rows is null).
+__device__ __forceinline__ uint32_t row_at(const uint32_t* rows, uint64_t i) { return rows ? rows[i] : (uint32_t)i; }
+
 __global__ void k_wedge_count(const uint64_t* off, const uint32_t* len, const uint32_t* mem, const uint32_t* vlen,
-                              uint32_t n, uint64_t* wedges) {
-  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+                              const uint32_t* rows, uint32_t n, uint64_t* wedges) {
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t r = row_at(rows, i);
     const uint64_t s = off[r];
     const uint32_t l = len[r];
     uint64_t w = 0;
-    for (uint32_t i = lane_id(); i < l; i += kWarp) w += vlen[mem[s + i]] - 1u;
+    for (uint32_t k = lane_id(); k < l; k += kWarp) w += vlen[mem[s + k]] - 1u;
     for (int d = 16; d; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
-    if (lane_id() == 0) wedges[r] = w;
+    if (lane_id() == 0) wedges[i] = w;
   }
 }
 
@@ -132,9 +138,10 @@ __global__ void k_wedge_count(const uint64_t* off, const uint32_t* len, const ui
 // r, written as key (b << 8) | pos into r's range of the chunk buffer.
 __global__ void k_expand(const uint64_t* h_off, const uint32_t* h_len, const uint32_t* h_mem, const uint64_t* v_off,
                          const uint32_t* v_len, const uint32_t* v_edge, const uint64_t* wedge_off,
-                         uint64_t chunk_base, uint32_t r0, uint32_t r1, uint32_t* keys) {
-  for (uint64_t r = r0 + global_warp(); r < r1; r += n_warps()) {
-    uint64_t pos = wedge_off[r] - chunk_base;
+                         const uint32_t* rows, uint64_t chunk_base, uint32_t r0, uint32_t r1, uint32_t* keys) {
+  for (uint64_t i = r0 + global_warp(); i < r1; i += n_warps()) {
+    const uint32_t r = row_at(rows, i);
+    uint64_t pos = wedge_off[i] - chunk_base;
     const uint64_t s = h_off[r];
     const uint32_t l = h_len[r];
     for (uint32_t p = 0; p < l; ++p) {
@@ -147,7 +154,7 @@ __global__ void k_expand(const uint64_t* h_off, const uint32_t* h_len, const uin
         bool keep = false;
         if (j < n) {
           b = v_edge[lo + j];
-          keep = (b != (uint32_t)r);
+          keep = (b != r);
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) keys[pos + __popc(m & lanemask_lt())] = (b << 8) | p;
@@ -197,8 +204,8 @@ __global__ void k_chunk_starts(const int* beg, const int* end, const uint32_t* k
   }
 }
 
-__global__ void k_chunk_emit(const int* beg, const int* end, const uint32_t* keys, uint32_t r0, uint32_t nrows,
-                             const uint64_t* local_off, const uint32_t* cnt, const uint32_t* starts,
+__global__ void k_chunk_emit(const int* beg, const int* end, const uint32_t* keys, const uint32_t* rows, uint32_t r0,
+                             uint32_t nrows, const uint64_t* local_off, const uint32_t* cnt, const uint32_t* starts,
                              uint64_t out_base, uint64_t* row_off,
                              uint32_t* row_len, uint32_t* nbr, uint8_t* ovl, uint64_t* pmask) {
   for (uint64_t r = global_warp(); r < nrows; r += n_warps()) {
@@ -207,8 +214,9 @@ __global__ void k_chunk_emit(const int* beg, const int* end, const uint32_t* key
     const uint32_t c = cnt[r];
     const uint64_t dst = out_base + lo;
     if (lane_id() == 0) {
-      row_off[r0 + r] = dst;
-      row_len[r0 + r] = c;
+      const uint32_t slot = row_at(rows, r0 + r);
+      row_off[slot] = dst;
+      row_len[slot] = c;
     }
     for (uint32_t k = lane_id(); k < c; k += kWarp) {
       const uint32_t st = starts[lo + k];
@@ -374,6 +382,8 @@ int build_h2v(hm_graph* g, const uint64_t* h_off, const uint32_t* h_mem, uint32_
   }
   g->h2v_len = static_cast<DArr<uint32_t>&&>(cnt);
   g->h2v_tail = total;
+  g->h2v_nnz = total;
+  g->cap_slots = n_edges;
   g->n_slots = n_edges;
   g->n_live = n_edges;
   const uint32_t words = (n_edges + 31) / 32;
@@ -383,11 +393,18 @@ int build_h2v(hm_graph* g, const uint64_t* h_off, const uint32_t* h_mem, uint32_
   return HM_OK;
 }
 
+// V2H from the live H2V rows (works on a compact or an updated arena: pairs
+// are placed by a scan of the row lengths).
 int build_v2h(hm_graph* g) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
-  const uint64_t nnz = g->h2v_tail;
   const uint32_t V = g->n_nodes;
+  DArr<uint64_t> pair_off;
+  HM_TRY(pair_off.alloc(ctx, (size_t)g->n_slots + 1));
+  HM_TRY(exclusive_scan(ctx, g->h2v_len.p, pair_off.p, g->n_slots));
+  uint64_t nnz = 0;
+  HM_CUDA(cudaMemcpyAsync(&nnz, pair_off.p + g->n_slots, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
   DArr<uint32_t> keys, vals, keys_out;
   HM_TRY(keys.alloc(ctx, nnz));
   HM_TRY(vals.alloc(ctx, nnz));
@@ -397,7 +414,7 @@ int build_v2h(hm_graph* g) {
   HM_CUDA(cudaMemsetAsync(g->v2h_len.p, 0, sizeof(uint32_t) * V, st));
   if (g->n_slots) {
     k_member_pairs<<<grid_for((uint64_t)g->n_slots * 32, kBlock), kBlock, 0, st>>>(
-        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->n_slots, keys.p, vals.p, g->v2h_len.p);
+        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->n_slots, pair_off.p, keys.p, vals.p, g->v2h_len.p);
     HM_LAUNCH_CHECK();
   }
   if (nnz) {
@@ -417,44 +434,57 @@ int build_v2h(hm_graph* g) {
   return HM_OK;
 }
 
-// H2H rows in chunks of the wedge stream: expand, segmented sort, run-length.
-int build_h2h_rows(hm_graph* g) {
+// H2H rows of the listed slots (all slots when d_rows is null), in chunks of
+// the wedge stream: expand, segmented sort, run-length. reserve(W) is called
+// once with an upper bound on the entries and returns the arena position
+// where the rows are written; *written receives the entries emitted.
+int h2h_rows_for(hm_graph* g, const uint32_t* d_rows, uint32_t n_rows,
+                 const std::function<int(uint64_t, uint64_t*)>& reserve, uint64_t* written) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
-  const uint32_t E = g->n_slots;
-  if (E >= (1u << 24))
-    return set_error(HM_ERR_LIMIT, "H2H build: %u hyperedge slots exceed the 2^24 limit of the packed sort key", E);
+  *written = 0;
+  if (g->n_slots >= (1u << 24))
+    return set_error(HM_ERR_LIMIT, "H2H: %u hyperedge slots exceed the 2^24 limit of the packed sort key", g->n_slots);
   DArr<uint64_t> wedges, woff;
-  HM_TRY(wedges.alloc(ctx, E));
-  HM_TRY(woff.alloc(ctx, (size_t)E + 1));
-  if (E) {
-    k_wedge_count<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
-                                                                       g->v2h_len.p, E, wedges.p);
+  HM_TRY(wedges.alloc(ctx, n_rows));
+  HM_TRY(woff.alloc(ctx, (size_t)n_rows + 1));
+  if (n_rows) {
+    k_wedge_count<<<grid_for((uint64_t)n_rows * 32, kBlock), kBlock, 0, st>>>(g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
+                                                                            g->v2h_len.p, d_rows, n_rows, wedges.p);
     HM_LAUNCH_CHECK();
   }
-  HM_TRY(exclusive_scan(ctx, wedges.p, woff.p, E));
-  std::vector<uint64_t> hw((size_t)E + 1);
-  HM_CUDA(cudaMemcpyAsync(hw.data(), woff.p, sizeof(uint64_t) * ((size_t)E + 1), cudaMemcpyDeviceToHost, st));
+  HM_TRY(exclusive_scan(ctx, wedges.p, woff.p, n_rows));
+  std::vector<uint64_t> hw((size_t)n_rows + 1);
+  HM_CUDA(cudaMemcpyAsync(hw.data(), woff.p, sizeof(uint64_t) * ((size_t)n_rows + 1), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
   wedges.release();
-  const uint64_t W = hw[E];
-  // The arena is sized by the wedge count, an upper bound on the entries.
-  HM_TRY(g->h2h_off.alloc(ctx, (size_t)E + 1));
-  HM_TRY(g->h2h_len.alloc(ctx, E));
-  HM_TRY(g->h2h_nbr.alloc(ctx, W));
-  HM_TRY(g->h2h_ovl.alloc(ctx, W));
-  HM_TRY(g->h2h_mask.alloc(ctx, W));
-  if (E == 0 || W == 0) {
-    if (E) HM_CUDA(cudaMemsetAsync(g->h2h_len.p, 0, sizeof(uint32_t) * E, st));
-    HM_CUDA(cudaMemsetAsync(g->h2h_off.p, 0, sizeof(uint64_t) * ((size_t)E + 1), st));
-    g->h2h_tail = 0;
-    g->h2h_nnz = 0;
+  const uint64_t W = hw[n_rows];
+  uint64_t base = 0;
+  HM_TRY(reserve(W, &base));
+  if (n_rows == 0) return HM_OK;
+  if (W == 0) {
+    // every listed row is empty
+    DArr<uint32_t> zero;
+    HM_TRY(zero.alloc(ctx, n_rows));
+    HM_CUDA(cudaMemsetAsync(zero.p, 0, sizeof(uint32_t) * n_rows, st));
+    DArr<int> beg, end;
+    DArr<uint64_t> loff;
+    HM_TRY(beg.alloc(ctx, n_rows));
+    HM_TRY(end.alloc(ctx, n_rows));
+    HM_TRY(loff.alloc(ctx, (size_t)n_rows + 1));
+    HM_CUDA(cudaMemsetAsync(beg.p, 0, sizeof(int) * n_rows, st));
+    HM_CUDA(cudaMemsetAsync(end.p, 0, sizeof(int) * n_rows, st));
+    HM_CUDA(cudaMemsetAsync(loff.p, 0, sizeof(uint64_t) * ((size_t)n_rows + 1), st));
+    k_chunk_emit<<<grid_for((uint64_t)n_rows * 32, kBlock), kBlock, 0, st>>>(
+        beg.p, end.p, nullptr, d_rows, 0, n_rows, loff.p, zero.p, nullptr, base, g->h2h_off.p, g->h2h_len.p,
+        g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
+    HM_LAUNCH_CHECK();
     return HM_OK;
   }
   uint64_t chunk_cap = std::min<uint64_t>(W, 1ull << 28);
   uint64_t max_row = 0;
-  for (uint32_t r = 0; r < E; ++r) max_row = std::max(max_row, hw[r + 1] - hw[r]);
-  if (max_row >= (1ull << 31)) return set_error(HM_ERR_LIMIT, "H2H build: one row has %llu wedges", (unsigned long long)max_row);
+  for (uint32_t r = 0; r < n_rows; ++r) max_row = std::max(max_row, hw[r + 1] - hw[r]);
+  if (max_row >= (1ull << 31)) return set_error(HM_ERR_LIMIT, "H2H: one row has %llu wedges", (unsigned long long)max_row);
   chunk_cap = std::max(chunk_cap, max_row);
   DArr<uint32_t> kin, kout, starts, cnt;
   DArr<int> beg, end;
@@ -462,26 +492,25 @@ int build_h2h_rows(hm_graph* g) {
   HM_TRY(kin.alloc(ctx, chunk_cap));
   HM_TRY(kout.alloc(ctx, chunk_cap));
   HM_TRY(starts.alloc(ctx, chunk_cap));
-  // rows per chunk are bounded by E
-  HM_TRY(cnt.alloc(ctx, E));
-  HM_TRY(beg.alloc(ctx, E));
-  HM_TRY(end.alloc(ctx, E));
-  HM_TRY(loff.alloc(ctx, (size_t)E + 1));
+  HM_TRY(cnt.alloc(ctx, n_rows));
+  HM_TRY(beg.alloc(ctx, n_rows));
+  HM_TRY(end.alloc(ctx, n_rows));
+  HM_TRY(loff.alloc(ctx, (size_t)n_rows + 1));
   DArr<uint8_t> sort_tmp;
   size_t sort_tb = 0;
-  uint64_t out_base = 0;
+  uint64_t out = 0;
   uint32_t r0 = 0;
-  while (r0 < E) {
+  while (r0 < n_rows) {
     uint32_t r1 = r0;
-    while (r1 < E && hw[r1 + 1] - hw[r0] <= chunk_cap) ++r1;
+    while (r1 < n_rows && hw[r1 + 1] - hw[r0] <= chunk_cap) ++r1;
     const uint32_t nrows = r1 - r0;
-    const uint64_t base = hw[r0];
-    const uint64_t nk = hw[r1] - base;
+    const uint64_t cbase = hw[r0];
+    const uint64_t nk = hw[r1] - cbase;
     k_expand<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(
-        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->v2h_off.p, g->v2h_len.p, g->v2h_edge.p, woff.p, base, r0, r1,
-        kin.p);
+        g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, g->v2h_off.p, g->v2h_len.p, g->v2h_edge.p, woff.p, d_rows, cbase,
+        r0, r1, kin.p);
     HM_LAUNCH_CHECK();
-    k_chunk_bounds<<<grid_for(nrows, kBlock), kBlock, 0, st>>>(woff.p, base, r0, r1, beg.p, end.p);
+    k_chunk_bounds<<<grid_for(nrows, kBlock), kBlock, 0, st>>>(woff.p, cbase, r0, r1, beg.p, end.p);
     HM_LAUNCH_CHECK();
     if (nk) {
       size_t tb = 0;
@@ -500,18 +529,38 @@ int build_h2h_rows(hm_graph* g) {
                                                                              starts.p);
     HM_LAUNCH_CHECK();
     k_chunk_emit<<<grid_for((uint64_t)nrows * 32, kBlock), kBlock, 0, st>>>(
-        beg.p, end.p, kout.p, r0, nrows, loff.p, cnt.p, starts.p, out_base, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
+        beg.p, end.p, kout.p, d_rows, r0, nrows, loff.p, cnt.p, starts.p, base + out, g->h2h_off.p, g->h2h_len.p,
+        g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
     HM_LAUNCH_CHECK();
     uint64_t chunk_total = 0;
     HM_CUDA(cudaMemcpyAsync(&chunk_total, loff.p + nrows, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
-    out_base += chunk_total;
+    out += chunk_total;
     r0 = r1;
   }
-  HM_CUDA(cudaMemcpyAsync(g->h2h_off.p + E, &out_base, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-  HM_CUDA(cudaStreamSynchronize(st));
-  g->h2h_tail = out_base;
-  g->h2h_nnz = out_base;
+  *written = out;
+  return HM_OK;
+}
+
+int build_h2h_rows(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  const uint32_t E = g->n_slots;
+  HM_TRY(g->h2h_off.alloc(ctx, (size_t)E + 1));
+  HM_TRY(g->h2h_len.alloc(ctx, E));
+  HM_CUDA(cudaMemsetAsync(g->h2h_len.p, 0, sizeof(uint32_t) * (E ? E : 1), ctx->stream));
+  auto reserve = [&](uint64_t W, uint64_t* base) -> int {
+    // the arena is sized by the wedge count, an upper bound on the entries
+    HM_TRY(g->h2h_nbr.alloc(ctx, W));
+    HM_TRY(g->h2h_ovl.alloc(ctx, W));
+    HM_TRY(g->h2h_mask.alloc(ctx, W));
+    g->h2h_cap = W;
+    *base = 0;
+    return HM_OK;
+  };
+  uint64_t written = 0;
+  HM_TRY(h2h_rows_for(g, nullptr, E, reserve, &written));
+  g->h2h_tail = written;
+  g->h2h_nnz = written;
   return HM_OK;
 }
 

@@ -73,6 +73,9 @@ _lib.bind(
         "hm_count_static30": (C.c_int, [vp, u64p]),
         "hm_count_static30_shard": (C.c_int, [vp, C.c_uint32, C.c_uint32, u64p]),
         "hm_graph_traffic": (C.c_int, [vp, C.POINTER(Traffic)]),
+        "hm_graph_apply_batch": (C.c_int, [vp, u32p, C.c_uint32, u64p, u32p, C.c_uint32, u32p, i64p]),
+        "hm_graph_live_ids": (C.c_int, [vp, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "hm_count_touching30": (C.c_int, [vp, u32p, C.c_uint32, u64p]),
         "hm_classify_static": (C.c_int, [C.c_int]),
         "hm_classify_temporal": (C.c_int, [C.c_int]),
     }
@@ -178,6 +181,34 @@ class Graph:
         t = Traffic()
         check(lib.hm_graph_traffic(self._h, C.byref(t)), "hm_graph_traffic")
         return t
+
+    def apply_batch(self, del_ids, ins_offsets=None, ins_members=None, delta: bool = True):
+        """Delete then insert; returns (assigned ids, 30-class delta or None)."""
+        d = np.ascontiguousarray(del_ids if del_ids is not None else [], dtype=np.uint32)
+        if ins_offsets is None:
+            ins_offsets, ins_members = np.zeros(1, np.uint64), np.zeros(0, np.uint32)
+        off, mem = _csr_arrays(ins_offsets, ins_members)
+        n_ins = len(off) - 1
+        ids = np.zeros(max(n_ins, 1), np.uint32)
+        dl = np.zeros(N_STATIC_CLASSES, np.int64) if delta else None
+        check(lib.hm_graph_apply_batch(self._h, ptr(d, C.c_uint32), len(d), ptr(off, C.c_uint64),
+                                       ptr(mem if len(mem) else np.zeros(1, np.uint32), C.c_uint32), n_ins,
+                                       ptr(ids, C.c_uint32), ptr(dl, C.c_int64)), "hm_graph_apply_batch")
+        return ids[:n_ins].copy(), dl
+
+    def live_ids(self) -> np.ndarray:
+        n = C.c_uint32()
+        check(lib.hm_graph_live_ids(self._h, None, 0, C.byref(n)), "hm_graph_live_ids")
+        out = np.zeros(max(n.value, 1), np.uint32)
+        check(lib.hm_graph_live_ids(self._h, ptr(out, C.c_uint32), len(out), C.byref(n)), "hm_graph_live_ids")
+        return out[: n.value].copy()
+
+    def count_touching30(self, ids) -> np.ndarray:
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        out = np.zeros(N_STATIC_CLASSES, np.uint64)
+        check(lib.hm_count_touching30(self._h, ptr(ids, C.c_uint32), len(ids), ptr(out, C.c_uint64)),
+              "hm_count_touching30")
+        return out
 
     def query(self, ids) -> list[np.ndarray]:
         ids = np.ascontiguousarray(ids, dtype=np.uint32)
