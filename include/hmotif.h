@@ -194,6 +194,18 @@ int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]);
  * only when hyperedges repeat). */
 int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]);
 
+/* THyMe's 96 temporal h-motif counts of a temporal graph (built with
+ * timestamps) for the window delta: every event a and the connected triples
+ * of the projection of the events with t_a - delta <= t <= t_a that contain
+ * it, repeated node-sets collapsed into one hyperedge with several
+ * occurrences (THyMe-main/code/main_thymeP.cpp:155-368). Equal timestamps are
+ * ordered by input position. HM_ERR_LIMIT if an event has more than 2048
+ * distinct neighbours inside its window. There is no temporal counter of
+ * these 96 motifs in the reference's GPU code (its 3-layer strict-increasing
+ * kernel, temporalDynamicHMotif/src/temporal_count.cu:91-217, bins 30 classes
+ * of a different definition). */
+int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_MOTIFS]);
+
 /* Partial 30-class counts over one shard of the centres: the sum over
  * shard = 0 .. n_shards-1 equals hm_count_static30. One shard per GPU, each
  * GPU holding a replica of the graph, gives the multi-GPU count with a

@@ -53,8 +53,10 @@ extern "C" int hm_graph_build(hm_ctx* ctx, const uint64_t* offsets, const uint32
   static const uint64_t zero_off = 0;
   const uint64_t* off = n_edges ? offsets : &zero_off;
   int s = hm::build_h2v(g, off, members, n_edges);
-  if (s >= 0) s = hm::build_v2h(g);
-  if (s >= 0) s = hm::build_h2h_rows(g);
+  // a temporal graph only needs its member lists; the time-ordered index is
+  // built by the first temporal count
+  if (s >= 0 && !timestamps) s = hm::build_v2h(g);
+  if (s >= 0 && !timestamps) s = hm::build_h2h_rows(g);
   if (s >= 0 && timestamps) {
     s = g->ts.alloc(ctx, n_edges);
     if (s >= 0 && n_edges) {
@@ -111,8 +113,13 @@ extern "C" int hm_graph_timings(const hm_graph* g, hm_timings_t* t) {
   return HM_OK;
 }
 
+static int static_ok(const hm_graph* g) {
+  return g->temporal ? hm::set_error(HM_ERR_STATE, "static count: the graph is temporal; use hm_count_temporal") : HM_OK;
+}
+
 extern "C" int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]) {
   if (!g || !out30) return hm::set_error(HM_ERR_INVALID, "hm_count_static30: NULL argument");
+  HM_TRY(static_ok(g));
   CtxLock lock(g->ctx);
   return hm::count_static30(g, 0, 1, out30);
 }
@@ -120,12 +127,14 @@ extern "C" int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES
 extern "C" int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_shards,
                                        uint64_t out30[HM_N_STATIC_CLASSES]) {
   if (!g || !out30) return hm::set_error(HM_ERR_INVALID, "hm_count_static30_shard: NULL argument");
+  HM_TRY(static_ok(g));
   CtxLock lock(g->ctx);
   return hm::count_static30(g, shard, n_shards, out30);
 }
 
 extern "C" int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]) {
   if (!g || !out26) return hm::set_error(HM_ERR_INVALID, "hm_count_static: NULL argument");
+  HM_TRY(static_ok(g));
   uint64_t c30[30];
   CtxLock lock(g->ctx);
   HM_TRY(hm::count_static30(g, 0, 1, c30));
@@ -201,6 +210,7 @@ extern "C" int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32
 
 extern "C" int hm_count_touching30(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t out30[HM_N_STATIC_CLASSES]) {
   if (!g || !out30 || (n && !ids)) return hm::set_error(HM_ERR_INVALID, "hm_count_touching30: NULL argument");
+  HM_TRY(static_ok(g));
   std::vector<uint32_t> u(ids, ids + n);
   std::sort(u.begin(), u.end());
   u.erase(std::unique(u.begin(), u.end()), u.end());
@@ -244,4 +254,14 @@ extern "C" int hm_graph_live_ids(const hm_graph* g, uint32_t* out, uint32_t cap,
   *n_out = n;
   if (out && n > cap) return hm::set_error(HM_ERR_CAPACITY, "hm_graph_live_ids: %u live ids > capacity %u", n, cap);
   return HM_OK;
+}
+
+namespace hm {
+int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]);
+}
+
+extern "C" int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_MOTIFS]) {
+  if (!g || !out96) return hm::set_error(HM_ERR_INVALID, "hm_count_temporal: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::count_temporal96(g, delta, out96);
 }

@@ -145,9 +145,20 @@ struct hm_graph {
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool ev_ready = false;
 
-  // temporal (optional): timestamps per slot
+  // temporal (optional): timestamps per slot and the time-ordered index
   hm::DArr<int64_t> ts;
   bool temporal = false;
+  bool t_ready = false;
+  hm::DArr<uint32_t> t_order;   // position -> event (events by time, then index)
+  hm::DArr<int64_t> t_time;     // position -> time
+  hm::DArr<uint32_t> t_static;  // position -> static id (smallest event with the same node-set)
+  hm::DArr<uint32_t> t_prev;    // position -> previous position of the same static id
+  hm::DArr<uint64_t> t_ooff;    // static id -> its occurrence positions
+  hm::DArr<uint32_t> t_olen;
+  hm::DArr<uint32_t> t_opos;
+  hm::DArr<uint64_t> t_voff;    // node -> positions of the events containing it
+  hm::DArr<uint32_t> t_vlen;
+  hm::DArr<uint32_t> t_vpos;
 
   hm::PhaseTimes times;
 

@@ -84,6 +84,7 @@ __global__ void k_oriented_bytes(const uint64_t* poff, const uint32_t* plen, con
 
 extern "C" int hm_graph_traffic(hm_graph* g, hm_traffic_t* t) {
   if (!g || !t) return hm::set_error(HM_ERR_INVALID, "hm_graph_traffic: NULL argument");
+  if (g->temporal) return hm::set_error(HM_ERR_STATE, "hm_graph_traffic: the graph is temporal");
   std::lock_guard<std::mutex> lock(g->ctx->mu);
   cudaSetDevice(g->ctx->device);
   hm_ctx* ctx = g->ctx;

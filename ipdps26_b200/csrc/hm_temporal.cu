@@ -1,0 +1,602 @@
+// Exact temporal h-motif counting: THyMe's 96 motifs over a delta window.
+//
+// Reference semantics: THyMe+ (THyMe-main/code/main_thymeP.cpp:155-368).
+// Events (a node-set with a timestamp) are processed in time order; the
+// window of event a holds the events at most delta older (t + delta >= t_a).
+// Identical node-sets collapse into one static hyperedge carrying the times of
+// its occurrences (:164-179). For each event a, every connected static triple
+// (a, b, c) of the window projection that contains a is an instance; it adds
+// the number of occurrence pairs (b before c) to the motif of the order
+// (b, c, a) and the pairs (c before b) to the motif of (c, b, a) (:243-334).
+// Pairs of a's earlier occurrences with a neighbour give motifs 87-95, and
+// two earlier occurrences of a itself motif 96 (:337-367).
+//
+// Device layout (built once per graph): events sorted by (time, input
+// index); per position its static id (the smallest event index with the same
+// node-set) and the previous position of that static id; node -> positions
+// of the events containing it; static id -> positions of its occurrences.
+//
+// Kernel: one block per event a (position p), over the window [lo, p):
+//   1. neighbours b of a: walk the window occurrences of a's nodes, keep the
+//      first occurrence of each static id, and accumulate the overlap C_ab and
+//      the positions of a's members it contains (mask) in a shared hash;
+//   2. pairs {b, c} of neighbours: closed when b and c overlap (g from the
+//      masks), open at a otherwise;
+//   3. open at b: c reaches b through a node outside a and c misses a;
+//      counted once per (b, c) at their smallest shared node;
+//   4. motifs 87-96 from the occurrence lists.
+// Ties in time are ordered by input index (THyMe's order among equal times is
+// random, so parity covers strictly increasing times).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "hm_classes.h"
+#include "hm_device.h"
+
+namespace hm {
+namespace {
+
+constexpr unsigned kWarp = 32;
+constexpr unsigned kBlock = 256;
+constexpr unsigned kWarps = kBlock / kWarp;
+constexpr unsigned kSlots = 4096;       // neighbour hash slots
+constexpr unsigned kMaxNbrs = kSlots / 2; // neighbours of one event inside its window
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr uint32_t kNone = 0xffffffffu;
+
+__constant__ int8_t c_temporal[128];
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint64_t global_warp() { return ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint64_t n_warps() { return ((uint64_t)gridDim.x * blockDim.x) >> 5; }
+__device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+
+__device__ __forceinline__ int tclass(int s1, int s2, int s3, int c12, int c23, int c31, int g) {
+  return c_temporal[region_pattern(s1, s2, s3, c12, c23, c31, g)];
+}
+
+// ---- index construction --------------------------------------------------------
+
+__global__ void k_row_hash(const uint64_t* off, const uint32_t* len, const uint32_t* mem, uint32_t n, uint64_t* h) {
+  for (uint64_t r = gtid(); r < n; r += gstride()) {
+    uint64_t x = 0x9E3779B97F4A7C15ull ^ len[r];
+    const uint32_t* m = mem + off[r];
+    for (uint32_t i = 0; i < len[r]; ++i) {
+      x ^= m[i] + 0x9E3779B97F4A7C15ull + (x << 6) + (x >> 2);
+      x *= 0xBF58476D1CE4E5B9ull;
+    }
+    h[r] = x ^ (x >> 31);
+  }
+}
+
+__device__ __forceinline__ bool same_rows(const uint64_t* off, const uint32_t* len, const uint32_t* mem, uint32_t a,
+                                          uint32_t b) {
+  if (len[a] != len[b]) return false;
+  const uint32_t* x = mem + off[a];
+  const uint32_t* y = mem + off[b];
+  for (uint32_t i = 0; i < len[a]; ++i)
+    if (x[i] != y[i]) return false;
+  return true;
+}
+
+// Events sorted by (hash, index): the static id of an event is the first
+// event of its hash run with the same node-set.
+__global__ void k_static_ids(const uint64_t* hs, const uint32_t* ev, uint32_t n, const uint64_t* off,
+                             const uint32_t* len, const uint32_t* mem, uint32_t* sid) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    uint64_t s = i;
+    while (s > 0 && hs[s - 1] == hs[i]) --s;
+    uint32_t rep = ev[i];
+    for (uint64_t k = s; k < i; ++k)
+      if (same_rows(off, len, mem, ev[k], ev[i])) {
+        rep = ev[k];
+        break;
+      }
+    sid[ev[i]] = rep;
+  }
+}
+
+__global__ void k_time_keys(const int64_t* t, uint32_t n, uint64_t* key, uint32_t* idx) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    key[i] = (uint64_t)t[i] ^ 0x8000000000000000ull;  // order-preserving for signed times
+    idx[i] = (uint32_t)i;
+  }
+}
+
+__global__ void k_position_fields(const uint32_t* order, uint32_t n, const int64_t* t, const uint32_t* sid,
+                                  int64_t* tp, uint32_t* sp, uint32_t* occ_key, uint32_t* occ_val) {
+  for (uint64_t p = gtid(); p < n; p += gstride()) {
+    const uint32_t e = order[p];
+    tp[p] = t[e];
+    sp[p] = sid[e];
+    occ_key[p] = sid[e];
+    occ_val[p] = (uint32_t)p;
+  }
+}
+
+__global__ void k_prev_same(const uint32_t* key, const uint32_t* pos, uint32_t n, uint32_t* prev) {
+  for (uint64_t i = gtid(); i < n; i += gstride())
+    prev[pos[i]] = (i > 0 && key[i - 1] == key[i]) ? pos[i - 1] : kNone;
+}
+
+__global__ void k_count_keys(const uint32_t* key, uint32_t n, uint32_t* cnt) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) atomicAdd(&cnt[key[i]], 1u);
+}
+
+// (node, position) pairs in position order.
+__global__ void k_node_positions(const uint32_t* order, uint32_t n, const uint64_t* off, const uint32_t* len,
+                                 const uint32_t* mem, const uint64_t* pair_off, uint32_t* key, uint32_t* val,
+                                 uint32_t* node_cnt) {
+  for (uint64_t p = global_warp(); p < n; p += n_warps()) {
+    const uint32_t e = order[p];
+    const uint64_t s = off[e], d = pair_off[p];
+    for (uint32_t i = lane_id(); i < len[e]; i += kWarp) {
+      const uint32_t v = mem[s + i];
+      key[d + i] = v;
+      val[d + i] = (uint32_t)p;
+      atomicAdd(&node_cnt[v], 1u);
+    }
+  }
+}
+
+__global__ void k_gather_len(const uint32_t* order, uint32_t n, const uint32_t* len, uint32_t* out) {
+  for (uint64_t p = gtid(); p < n; p += gstride()) out[p] = len[order[p]];
+}
+
+__global__ void k_window_lo(const int64_t* t, uint32_t n, int64_t delta, uint32_t* lo) {
+  for (uint64_t p = gtid(); p < n; p += gstride()) {
+    const int64_t tp = t[p];
+    // first q with t[q] + delta >= t[p]
+    uint32_t l = 0, h = (uint32_t)p;
+    while (l < h) {
+      const uint32_t mid = (l + h) >> 1;
+      if (t[mid] + delta < tp) l = mid + 1;
+      else h = mid;
+    }
+    lo[p] = l;
+  }
+}
+
+// ---- counting --------------------------------------------------------------------
+
+struct TArgs {
+  uint32_t n;            // events
+  const uint32_t* order; // position -> event
+  const uint32_t* sp;    // position -> static id
+  const uint32_t* prev;  // position -> previous position of the same static id
+  const uint32_t* lo;    // position -> window start
+  const uint64_t* hoff;  // event -> members
+  const uint32_t* hlen;
+  const uint32_t* hmem;
+  const uint64_t* voff;  // node -> positions
+  const uint32_t* vlen;
+  const uint32_t* vpos;
+  const uint64_t* ooff;  // static id -> occurrence positions
+  const uint32_t* olen;
+  const uint32_t* opos;
+  unsigned int* queue;
+  unsigned long long* out;  // 96
+  int* overflow;
+};
+
+// [first, last) of the sorted list x[0..n) restricted to values in [lo, hi)
+__device__ __forceinline__ void range_in(const uint32_t* x, uint32_t n, uint32_t lo, uint32_t hi, uint32_t& first,
+                                         uint32_t& last) {
+  uint32_t l = 0, h = n;
+  while (l < h) {
+    const uint32_t m = (l + h) >> 1;
+    if (x[m] < lo) l = m + 1;
+    else h = m;
+  }
+  first = l;
+  h = n;
+  while (l < h) {
+    const uint32_t m = (l + h) >> 1;
+    if (x[m] < hi) l = m + 1;
+    else h = m;
+  }
+  last = l;
+}
+
+// pairs (x in X, y in Y) with x < y, both sorted ascending
+__device__ __forceinline__ uint64_t ordered_pairs(const uint32_t* X, uint32_t nx, const uint32_t* Y, uint32_t ny) {
+  if (nx == 1 && ny == 1) return X[0] < Y[0];
+  uint64_t c = 0;
+  uint32_t j = 0;
+  for (uint32_t i = 0; i < nx; ++i) {
+    while (j < ny && Y[j] <= X[i]) ++j;
+    c += ny - j;
+  }
+  return c;
+}
+
+// |X & Y| and the smallest shared value (kNone if none)
+__device__ __forceinline__ uint32_t overlap(const uint32_t* X, uint32_t nx, const uint32_t* Y, uint32_t ny,
+                                            uint32_t& first) {
+  uint32_t i = 0, j = 0, c = 0;
+  first = kNone;
+  while (i < nx && j < ny) {
+    const uint32_t x = X[i], y = Y[j];
+    if (x < y) ++i;
+    else if (y < x) ++j;
+    else {
+      if (!c) first = x;
+      ++c;
+      ++i;
+      ++j;
+    }
+  }
+  return c;
+}
+
+constexpr size_t kTemporalSmem = kSlots * (sizeof(unsigned long long) + 2 * sizeof(uint32_t)) + kMaxNbrs * sizeof(uint16_t);
+
+__global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
+  extern __shared__ unsigned long long tsm[];
+  unsigned long long* smask = tsm;                                     // kSlots
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kSlots);        // kSlots
+  uint32_t* scab = keys + kSlots;                                      // kSlots
+  uint16_t* la = reinterpret_cast<uint16_t*>(scab + kSlots);           // kMaxNbrs: slots of the neighbours
+  __shared__ unsigned long long cnt96[96];
+  __shared__ uint32_t s_item, s_nla;
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  for (unsigned k = threadIdx.x; k < 96; k += blockDim.x) cnt96[k] = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(A.queue, 1u);
+      s_nla = 0;
+    }
+    for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
+    __syncthreads();
+    const uint32_t p = s_item;
+    if (p >= A.n) break;
+    const uint32_t lo = A.lo[p];
+    const uint32_t ea = A.order[p];
+    const uint32_t sa = A.sp[p];
+    const uint32_t* am = A.hmem + A.hoff[ea];
+    const uint32_t asz = A.hlen[ea];
+    // 1. neighbours of a in the window, overlap and member-position mask
+    for (uint32_t i = w; i < asz; i += kWarps) {
+      const uint32_t v = am[i];
+      const uint32_t* vp = A.vpos + A.voff[v];
+      uint32_t f, l;
+      range_in(vp, A.vlen[v], lo, p, f, l);
+      for (uint32_t k = f + lane; k < l; k += kWarp) {
+        const uint32_t q = vp[k];
+        const uint32_t x = A.sp[q];
+        if (x == sa) continue;
+        const uint32_t pr = A.prev[q];
+        if (pr != kNone && pr >= lo) continue;  // not the first occurrence of x in the window
+        uint32_t h = (x * 2654435761u) >> (32 - 12);
+        for (uint32_t probe = 0;; ++probe) {
+          if (probe == kSlots) {  // table full: more neighbours than the window limit
+            atomicAdd(&s_nla, (uint32_t)kSlots);
+            break;
+          }
+          const uint32_t old = atomicCAS(&keys[h], kEmpty, x);
+          if (old == kEmpty) {
+            const uint32_t idx = atomicAdd(&s_nla, 1u);
+            if (idx < kMaxNbrs) la[idx] = (uint16_t)h;
+            scab[h] = 0;
+            smask[h] = 0;
+          }
+          if (old == kEmpty || old == x) break;
+          h = (h + 1) & (kSlots - 1);
+        }
+      }
+    }
+    __syncthreads();
+    // counts are added in a second sweep so that initialisation precedes them
+    for (uint32_t i = w; i < asz; i += kWarps) {
+      const uint32_t v = am[i];
+      const uint32_t* vp = A.vpos + A.voff[v];
+      uint32_t f, l;
+      range_in(vp, A.vlen[v], lo, p, f, l);
+      for (uint32_t k = f + lane; k < l; k += kWarp) {
+        const uint32_t q = vp[k];
+        const uint32_t x = A.sp[q];
+        if (x == sa) continue;
+        const uint32_t pr = A.prev[q];
+        if (pr != kNone && pr >= lo) continue;
+        uint32_t h = (x * 2654435761u) >> (32 - 12);
+        uint32_t probe = 0;
+        while (keys[h] != x && probe < kSlots) {
+          h = (h + 1) & (kSlots - 1);
+          ++probe;
+        }
+        if (probe == kSlots) continue;  // not stored (overflow is reported)
+        atomicAdd(&scab[h], 1u);
+        if (i < 64) atomicOr(&smask[h], 1ull << i);
+      }
+    }
+    __syncthreads();
+    const uint32_t nla = s_nla;
+    if (nla > kMaxNbrs) {
+      if (threadIdx.x == 0) atomicExch(A.overflow, 1);
+      continue;  // block-uniform; the whole count is reported as failed
+    }
+    const uint32_t* ao = A.opos + A.ooff[sa];
+    uint32_t af, al;
+    range_in(ao, A.olen[sa], lo, p, af, al);  // a's earlier occurrences in the window
+    const uint32_t ta_n = al - af;
+    // 2. pairs of neighbours
+    for (uint32_t i = w; i < nla; i += kWarps) {
+      const uint32_t hb = la[i];
+      const uint32_t b = keys[hb], cab = scab[hb];
+      const unsigned long long mb = smask[hb];
+      const uint32_t* bm = A.hmem + A.hoff[b];
+      const uint32_t bsz = A.hlen[b];
+      const uint32_t* bo = A.opos + A.ooff[b];
+      uint32_t bf, bl;
+      range_in(bo, A.olen[b], lo, p, bf, bl);
+      for (uint32_t j = i + 1 + lane; j < nla; j += kWarp) {
+        const uint32_t hc = la[j];
+        const uint32_t c = keys[hc], cac = scab[hc];
+        const unsigned long long mc = smask[hc];
+        const uint32_t* cm = A.hmem + A.hoff[c];
+        const uint32_t csz = A.hlen[c];
+        uint32_t first;
+        const uint32_t cbc = overlap(bm, bsz, cm, csz, first);
+        uint32_t g = 0;
+        if (cbc) {
+          if (asz <= 64) {
+            g = __popcll(mb & mc);
+          } else {
+            // |a & b & c| by merging a's members with the b & c shared list
+            uint32_t x = 0, y = 0, z = 0;
+            while (x < asz && y < bsz && z < csz) {
+              const uint32_t u = am[x], vv = bm[y], t = cm[z];
+              const uint32_t mx = max(u, max(vv, t));
+              if (u == mx && vv == mx && t == mx) { ++g; ++x; ++y; ++z; }
+              else { x += u < mx; y += vv < mx; z += t < mx; }
+            }
+          }
+        }
+        const uint32_t* co = A.opos + A.ooff[c];
+        uint32_t cf, cl;
+        range_in(co, A.olen[c], lo, p, cf, cl);
+        const uint32_t nb = bl - bf, nc = cl - cf;
+        const uint64_t bc = ordered_pairs(bo + bf, nb, co + cf, nc);
+        const uint64_t cb = (uint64_t)nb * nc - bc;
+        const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, (int)cac, (int)cab, (int)g);
+        const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, (int)cac, (int)g);
+        if (bc && kbc >= 0) atomicAdd(&cnt96[kbc], (unsigned long long)bc);
+        if (cb && kcb >= 0) atomicAdd(&cnt96[kcb], (unsigned long long)cb);
+      }
+      // 4. motifs 87-95 for the pair (a, b)
+      if (lane == 0) {
+        const uint32_t tb_n = bl - bf;
+        const uint64_t ab = ordered_pairs(ao + af, ta_n, bo + bf, tb_n);
+        const uint64_t ba = (uint64_t)ta_n * tb_n - ab;
+        const uint64_t bb = (uint64_t)tb_n * (tb_n ? tb_n - 1 : 0) / 2;
+        const int kab = tclass((int)asz, (int)bsz, (int)asz, (int)cab, (int)cab, (int)asz, (int)cab);
+        const int kba = tclass((int)bsz, (int)asz, (int)asz, (int)cab, (int)asz, (int)cab, (int)cab);
+        const int kbb = tclass((int)bsz, (int)bsz, (int)asz, (int)bsz, (int)cab, (int)cab, (int)cab);
+        if (ab && kab >= 0) atomicAdd(&cnt96[kab], (unsigned long long)ab);
+        if (ba && kba >= 0) atomicAdd(&cnt96[kba], (unsigned long long)ba);
+        if (bb && kbb >= 0) atomicAdd(&cnt96[kbb], (unsigned long long)bb);
+      }
+    }
+    // 3. open at b: c meets b outside a and misses a
+    for (uint32_t i = w; i < nla; i += kWarps) {
+      const uint32_t hb = la[i];
+      const uint32_t b = keys[hb], cab = scab[hb];
+      const uint32_t* bm = A.hmem + A.hoff[b];
+      const uint32_t bsz = A.hlen[b];
+      const uint32_t* bo = A.opos + A.ooff[b];
+      uint32_t bf, bl;
+      range_in(bo, A.olen[b], lo, p, bf, bl);
+      for (uint32_t kk = 0; kk < bsz; ++kk) {
+        const uint32_t v = bm[kk];
+        // skip nodes of a (a's members are sorted)
+        uint32_t l2 = 0, h2 = asz;
+        while (l2 < h2) {
+          const uint32_t m = (l2 + h2) >> 1;
+          if (am[m] < v) l2 = m + 1;
+          else h2 = m;
+        }
+        if (l2 < asz && am[l2] == v) continue;
+        const uint32_t* vp = A.vpos + A.voff[v];
+        uint32_t f, l;
+        range_in(vp, A.vlen[v], lo, p, f, l);
+        for (uint32_t k = f + lane; k < l; k += kWarp) {
+          const uint32_t q = vp[k];
+          const uint32_t c = A.sp[q];
+          if (c == b || c == sa) continue;
+          const uint32_t pr = A.prev[q];
+          if (pr != kNone && pr >= lo) continue;
+          // c must miss a: not a neighbour of a
+          uint32_t h = (c * 2654435761u) >> (32 - 12);
+          bool nbr_of_a = false;
+          for (;;) {
+            const uint32_t kh = keys[h];
+            if (kh == c) { nbr_of_a = true; break; }
+            if (kh == kEmpty) break;
+            h = (h + 1) & (kSlots - 1);
+          }
+          if (nbr_of_a) continue;
+          const uint32_t* cm = A.hmem + A.hoff[c];
+          const uint32_t csz = A.hlen[c];
+          uint32_t first;
+          const uint32_t cbc = overlap(bm, bsz, cm, csz, first);
+          if (first != v) continue;  // counted at the smallest shared node
+          const uint32_t* co = A.opos + A.ooff[c];
+          uint32_t cf, cl;
+          range_in(co, A.olen[c], lo, p, cf, cl);
+          const uint32_t nb = bl - bf, nc = cl - cf;
+          const uint64_t bc = ordered_pairs(bo + bf, nb, co + cf, nc);
+          const uint64_t cb = (uint64_t)nb * nc - bc;
+          const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, 0, (int)cab, 0);
+          const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, 0, 0);
+          if (bc && kbc >= 0) atomicAdd(&cnt96[kbc], (unsigned long long)bc);
+          if (cb && kcb >= 0) atomicAdd(&cnt96[kcb], (unsigned long long)cb);
+        }
+      }
+    }
+    // 4. motif 96: two earlier occurrences of a
+    if (threadIdx.x == 0 && ta_n >= 2) atomicAdd(&cnt96[95], (unsigned long long)ta_n * (ta_n - 1) / 2);
+    __syncthreads();
+  }
+  __syncthreads();
+  for (unsigned k = threadIdx.x; k < 96; k += blockDim.x)
+    if (cnt96[k]) atomicAdd(&A.out[k], cnt96[k]);
+}
+
+template <class K, class V>
+int sort_pairs(hm_ctx* ctx, const K* kin, K* kout, const V* vin, V* vout, uint64_t n, int end_bit) {
+  size_t tb = 0;
+  HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int64_t)n, 0, end_bit, ctx->stream));
+  DArr<uint8_t> tmp;
+  HM_TRY(tmp.alloc(ctx, tb));
+  HM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, kin, kout, vin, vout, (int64_t)n, 0, end_bit, ctx->stream));
+  return HM_OK;
+}
+
+}  // namespace
+
+// Builds the time-ordered index of a temporal graph (once).
+static int build_temporal_index(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = g->n_slots;
+  static bool table_ready = false;
+  if (!table_ready) {
+    int8_t inv[128];
+    for (int i = 0; i < 128; ++i) inv[i] = -1;
+    for (int m = 0; m < HM_N_TEMPORAL_MOTIFS; ++m) inv[kTemporalMotifPattern[m]] = (int8_t)m;
+    HM_CUDA(cudaMemcpyToSymbol(c_temporal, inv, sizeof(inv)));
+    table_ready = true;
+  }
+  // static ids
+  DArr<uint64_t> hs, hs_sorted;
+  DArr<uint32_t> ev, ev_sorted, sid;
+  HM_TRY(hs.alloc(ctx, n));
+  HM_TRY(hs_sorted.alloc(ctx, n));
+  HM_TRY(ev.alloc(ctx, n));
+  HM_TRY(ev_sorted.alloc(ctx, n));
+  HM_TRY(sid.alloc(ctx, n));
+  k_row_hash<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p, n, hs.p);
+  HM_LAUNCH_CHECK();
+  {
+    std::vector<uint32_t> iota(n);
+    for (uint32_t i = 0; i < n; ++i) iota[i] = i;
+    HM_CUDA(cudaMemcpyAsync(ev.p, iota.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+  }
+  HM_TRY(sort_pairs(ctx, hs.p, hs_sorted.p, ev.p, ev_sorted.p, n, 64));
+  k_static_ids<<<grid_for(n, kBlock), kBlock, 0, st>>>(hs_sorted.p, ev_sorted.p, n, g->h2v_off.p, g->h2v_len.p,
+                                                        g->h2v_mem.p, sid.p);
+  HM_LAUNCH_CHECK();
+  // time order
+  DArr<uint64_t> tk, tk_sorted;
+  HM_TRY(tk.alloc(ctx, n));
+  HM_TRY(tk_sorted.alloc(ctx, n));
+  HM_TRY(g->t_order.alloc(ctx, n));
+  k_time_keys<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->ts.p, n, tk.p, ev.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(sort_pairs(ctx, tk.p, tk_sorted.p, ev.p, g->t_order.p, n, 64));
+  HM_TRY(g->t_time.alloc(ctx, n));
+  HM_TRY(g->t_static.alloc(ctx, n));
+  DArr<uint32_t> okey, oval, okey_s;
+  HM_TRY(okey.alloc(ctx, n));
+  HM_TRY(oval.alloc(ctx, n));
+  HM_TRY(okey_s.alloc(ctx, n));
+  HM_TRY(g->t_opos.alloc(ctx, n));
+  k_position_fields<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_order.p, n, g->ts.p, sid.p, g->t_time.p,
+                                                             g->t_static.p, okey.p, oval.p);
+  HM_LAUNCH_CHECK();
+  int eb = 1;
+  while (eb < 32 && (1ull << eb) < n) ++eb;
+  HM_TRY(sort_pairs(ctx, okey.p, okey_s.p, oval.p, g->t_opos.p, n, eb));
+  HM_TRY(g->t_prev.alloc(ctx, n));
+  k_prev_same<<<grid_for(n, kBlock), kBlock, 0, st>>>(okey_s.p, g->t_opos.p, n, g->t_prev.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(g->t_olen.alloc(ctx, n));
+  HM_CUDA(cudaMemsetAsync(g->t_olen.p, 0, sizeof(uint32_t) * n, st));
+  k_count_keys<<<grid_for(n, kBlock), kBlock, 0, st>>>(okey_s.p, n, g->t_olen.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(g->t_ooff.alloc(ctx, (size_t)n + 1));
+  HM_TRY(exclusive_scan(ctx, g->t_olen.p, g->t_ooff.p, n));
+  // node -> positions
+  DArr<uint32_t> plen;
+  DArr<uint64_t> poff;
+  HM_TRY(plen.alloc(ctx, n));
+  HM_TRY(poff.alloc(ctx, (size_t)n + 1));
+  k_gather_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_order.p, n, g->h2v_len.p, plen.p);
+  HM_LAUNCH_CHECK();
+  HM_TRY(exclusive_scan(ctx, plen.p, poff.p, n));
+  uint64_t nnz = 0;
+  HM_CUDA(cudaMemcpyAsync(&nnz, poff.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  const uint32_t V = g->n_nodes;
+  DArr<uint32_t> nk, nv, nk_s;
+  HM_TRY(nk.alloc(ctx, nnz));
+  HM_TRY(nv.alloc(ctx, nnz));
+  HM_TRY(nk_s.alloc(ctx, nnz));
+  HM_TRY(g->t_vpos.alloc(ctx, nnz));
+  HM_TRY(g->t_vlen.alloc(ctx, V));
+  HM_CUDA(cudaMemsetAsync(g->t_vlen.p, 0, sizeof(uint32_t) * V, st));
+  k_node_positions<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(g->t_order.p, n, g->h2v_off.p, g->h2v_len.p,
+                                                                         g->h2v_mem.p, poff.p, nk.p, nv.p,
+                                                                         g->t_vlen.p);
+  HM_LAUNCH_CHECK();
+  int vb = 1;
+  while (vb < 32 && (1ull << vb) < V) ++vb;
+  if (nnz) HM_TRY(sort_pairs(ctx, nk.p, nk_s.p, nv.p, g->t_vpos.p, nnz, vb));
+  HM_TRY(g->t_voff.alloc(ctx, (size_t)V + 1));
+  HM_TRY(exclusive_scan(ctx, g->t_vlen.p, g->t_voff.p, V));
+  HM_CUDA(cudaStreamSynchronize(st));
+  g->t_ready = true;
+  return HM_OK;
+}
+
+int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < 96; ++k) out96[k] = 0;
+  if (!g->temporal) return set_error(HM_ERR_STATE, "temporal count: the graph has no timestamps");
+  if (delta < 0) return set_error(HM_ERR_INVALID, "temporal count: delta must be >= 0");
+  const uint32_t n = g->n_slots;
+  if (!n) return HM_OK;
+  if (!g->t_ready) HM_TRY(build_temporal_index(g));
+  DArr<uint32_t> lo;
+  DArr<unsigned long long> acc;
+  HM_TRY(lo.alloc(ctx, n));
+  HM_TRY(acc.alloc(ctx, 98));
+  HM_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 98, st));
+  cudaEvent_t e0, e1;
+  HM_CUDA(cudaEventCreate(&e0));
+  HM_CUDA(cudaEventCreate(&e1));
+  HM_CUDA(cudaEventRecord(e0, st));
+  k_window_lo<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_time.p, n, delta, lo.p);
+  HM_LAUNCH_CHECK();
+  TArgs A{n, g->t_order.p, g->t_static.p, g->t_prev.p, lo.p, g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
+          g->t_voff.p, g->t_vlen.p, g->t_vpos.p, g->t_ooff.p, g->t_olen.p, g->t_opos.p,
+          reinterpret_cast<unsigned int*>(acc.p + 96), acc.p, reinterpret_cast<int*>(acc.p + 97)};
+  static bool attr = false;
+  if (!attr) {
+    HM_CUDA(cudaFuncSetAttribute(k_temporal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTemporalSmem));
+    attr = true;
+  }
+  k_temporal<<<std::min<unsigned>((unsigned)ctx->n_sms * 3, n), kBlock, kTemporalSmem, st>>>(A);
+  HM_LAUNCH_CHECK();
+  HM_CUDA(cudaEventRecord(e1, st));
+  unsigned long long h[98];
+  HM_CUDA(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g->times.temporal_ms = ms;
+  if (h[97])
+    return set_error(HM_ERR_LIMIT, "temporal count: an event has more than %u neighbours inside its window",
+                     kMaxNbrs);
+  for (int k = 0; k < 96; ++k) out96[k] = h[k];
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -76,6 +76,7 @@ _lib.bind(
         "hm_graph_apply_batch": (C.c_int, [vp, u32p, C.c_uint32, u64p, u32p, C.c_uint32, u32p, i64p]),
         "hm_graph_live_ids": (C.c_int, [vp, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_count_touching30": (C.c_int, [vp, u32p, C.c_uint32, u64p]),
+        "hm_count_temporal": (C.c_int, [vp, C.c_int64, u64p]),
         "hm_classify_static": (C.c_int, [C.c_int]),
         "hm_classify_temporal": (C.c_int, [C.c_int]),
     }
@@ -202,6 +203,11 @@ class Graph:
         out = np.zeros(max(n.value, 1), np.uint32)
         check(lib.hm_graph_live_ids(self._h, ptr(out, C.c_uint32), len(out), C.byref(n)), "hm_graph_live_ids")
         return out[: n.value].copy()
+
+    def count_temporal(self, delta: int) -> np.ndarray:
+        out = np.zeros(N_TEMPORAL_MOTIFS, np.uint64)
+        check(lib.hm_count_temporal(self._h, int(delta), ptr(out, C.c_uint64)), "hm_count_temporal")
+        return out
 
     def count_touching30(self, ids) -> np.ndarray:
         ids = np.ascontiguousarray(ids, dtype=np.uint32)

@@ -1,0 +1,69 @@
+"""Temporal 96-motif counts on the GPU against THyMe's own outputs (golden
+fixtures) and the CPU oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.helpers import csr, digest, load_golden, random_graph, temporal_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(load_golden("temporal")))
+def test_temporal_matches_thyme_golden(ctx, name):
+    from ipdps26_b200 import engine
+
+    rec = load_golden("temporal")[name]
+    h = temporal_case(rec["params"])
+    assert digest(h) == rec["sha256"]
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        for d, want in rec["counts96"].items():
+            assert g.count_temporal(int(d)).tolist() == want, d
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_temporal_matches_oracle_random(ctx, seed):
+    from ipdps26_b200 import engine
+
+    rng = np.random.default_rng(50 + seed)
+    n_nodes = int(rng.integers(6, 30))
+    off, mem = random_graph(rng, int(rng.integers(5, 120)), n_nodes, int(rng.integers(2, 6)), p_repeat=0.2)
+    rows = [mem[off[i]:off[i + 1]].tolist() for i in range(len(off) - 1)]
+    for i in range(0, len(rows), 4):  # repeated node-sets
+        rows[i] = rows[max(0, i - 2)]
+    off, mem = csr(rows)
+    times = np.cumsum(rng.integers(1, 30, size=len(rows))).astype(np.int64)
+    perm = rng.permutation(len(rows))  # input order differs from time order
+    rows = [rows[i] for i in perm]
+    times = times[perm]
+    off, mem = csr(rows)
+    with engine.Graph(ctx, off, mem, n_nodes, times) as g:
+        for delta in (0, 20, 100, 10_000):
+            want = oracle.temporal96(off, mem, times, delta)
+            assert g.count_temporal(delta).tolist() == want.tolist(), delta
+
+
+def test_temporal_graph_is_not_static(ctx):
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HmError
+
+    off, mem = csr([[0, 1], [1, 2]])
+    with engine.Graph(ctx, off, mem, 3, np.array([1, 2], np.int64)) as g:
+        with pytest.raises(HmError) as e:
+            g.count_static30()
+        assert e.value.status == -7
+        with pytest.raises(HmError):
+            g.apply_batch([0])
+        with pytest.raises(HmError) as e:
+            g.count_temporal(-1)
+        assert e.value.status == -1
+
+
+def test_temporal_c4_laws(ctx):
+    from ipdps26_b200 import engine, gen
+
+    h = gen.temporal(gen.config4(seed=8, n_nodes=1500, n_edges=3000), span=600_000)
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        for delta in (1000, 10_000):
+            want = oracle.temporal96(h.offsets, h.members, h.timestamps, delta)
+            assert g.count_temporal(delta).tolist() == want.tolist(), delta
