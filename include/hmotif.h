@@ -194,6 +194,20 @@ int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]);
  * only when hyperedges repeat). */
 int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]);
 
+/* The same counts as hm_count_touching30, for callers that cannot allocate
+ * device memory while they run (a serving thread that must not block on the
+ * allocator or fail for want of memory mid-request, code held to a fixed
+ * memory reservation). No counterpart in the reference. d_ids (n ids) and
+ * d_out30 (30 uint64) are device buffers owned by the caller; stream is a
+ * cudaStream_t (NULL: the context stream). All scratch lives in one 8 MiB
+ * device array that the library sets aside when it is loaded: graphs of at
+ * most 2^21 hyperedge slots, at most 2^20 distinct ids per call. The first
+ * call on a device looks the array up and configures the kernels; make it
+ * before any stream capture. Calls share the array, so calls that overlap on
+ * the GPU race: serialise them. Returns when the counts are written;
+ * HM_ERR_NOT_LIVE if an id is not a live hyperedge (the others are counted). */
+int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t* d_out30, void* stream);
+
 /* THyMe's 96 temporal h-motif counts of a temporal graph (built with
  * timestamps) for the window delta: every event a and the connected triples
  * of the projection of the events with t_a - delta <= t <= t_a that contain
