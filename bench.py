@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    ap.add_argument("--update-batches", type=int, default=20,
+                    help="config-3 batches applied to the resident graph after the static steps (0: skip)")
+    ap.add_argument("--no-update-check", action="store_true",
+                    help="skip the full recount that checks the summed deltas")
+    ap.add_argument("--no-temporal", action="store_true")
     return ap.parse_args()
 
 
@@ -173,6 +178,61 @@ def cpu_baseline(h, budget_s: float):
             "sample": f"MoCHy main_exact_par, first {n} hyperedges of the workload (same laws and node universe), "
                       f"{triples} triples (26 motifs) in {wall:.2f} s wall including its file parse",
             "wall_s": wall, "sample_hyperedges": n}
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def update_section(args, g, p, counts30):
+    """Config 3: update batches on the resident config-2 graph, each with its
+    exact incremental recount; the summed deltas are checked against one full
+    recount at the end. Batch sizes are log-uniform in [1000, 100000] edits,
+    80 % insertions drawn from the config-2 laws, 20 % deletions uniform over
+    the live hyperedges (seed 2)."""
+    from ipdps26_b200 import gen
+
+    rng = np.random.default_rng(2)
+    total = counts30.astype(np.int64).copy()
+    wall, dev, sizes = [], [], []
+    for b in range(args.update_batches):
+        n_edits = int(np.exp(rng.uniform(np.log(1_000), np.log(100_000))))
+        live = g.live_ids()
+        dels, ins = gen.batch(p, 2_000_000 + b, live, n_edits, 0.8)
+        t0 = time.perf_counter()
+        _, delta = g.apply_batch(dels, ins.offsets, ins.members)
+        wall.append(time.perf_counter() - t0)
+        dev.append(g.timings().update_ms / 1000.0)
+        sizes.append(n_edits)
+        total += delta
+    out = {"batches": len(wall), "edits_min": min(sizes), "edits_max": max(sizes),
+           "edits_total": int(sum(sizes)), "p50_ms": 1000 * pct(wall, 50), "p99_ms": 1000 * pct(wall, 99),
+           "device_p50_ms": 1000 * pct(dev, 50), "device_p99_ms": 1000 * pct(dev, 99),
+           "batches_per_s": len(wall) / sum(wall), "edits_per_s": sum(sizes) / sum(wall),
+           "form": "plain per-call (hm_graph_apply_batch with the exact delta)"}
+    if not args.no_update_check:
+        full = g.count_static30().astype(np.int64)
+        out["delta_sum_equals_full_recount"] = bool(np.array_equal(full, total))
+    return out
+
+
+def temporal_section(ctx):
+    """Config 4: THyMe's 96 temporal motifs over 500K bursty events, for
+    delta in {1e3, 1e4, 1e5} (device time of one count each)."""
+    from ipdps26_b200 import engine, gen
+
+    h = gen.temporal(gen.config4())
+    res = {"events": h.n_edges, "workload": "config4 seed=3 200K nodes, Zipf(1.2), bursty span 1e8"}
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        for d in (1_000, 10_000, 100_000):
+            c = g.count_temporal(d)
+            c = g.count_temporal(d)
+            ms = g.timings().temporal_ms
+            res[f"delta_{d}"] = {"ms": ms, "instances_counted": int(c.sum()),
+                                 "temporal_triples_per_s": float(c.sum()) / (ms / 1000.0)}
+    return res
 
 
 def reference_arm(args, rank, world):
@@ -313,6 +373,12 @@ def engine_arm(args, rank, world, local_rank):
         base = None
         if world == 1 and not args.no_cpu_baseline:
             base = cpu_baseline(h, args.cpu_sample_seconds)
+        updates = None
+        if args.update_batches > 0:
+            updates = update_section(args, g, p, counts)
+        temporal = None
+        if not args.no_temporal:
+            temporal = temporal_section(ctx)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
@@ -322,6 +388,7 @@ def engine_arm(args, rank, world, local_rank):
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
                       "device_gb": info.device_bytes / 1e9},
+            "update_batches": updates, "temporal": temporal,
         }
         print(json.dumps(result), flush=True)
     g.close()

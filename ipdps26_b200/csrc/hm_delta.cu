@@ -3,7 +3,8 @@
 // for the inserted ids on the new graph minus it for the deleted ids on the
 // old graph.
 //
-// Same open/closed split as the static count (hm_static.cu):
+// Same open/closed split as the static count (hm_static.cu), with its
+// bucketized hash, unrolled probes and star fast path:
 //   * open phase over the centres that are marked or adjacent to a marked
 //     hyperedge: pairs {b, c} of the centre's neighbours that contain a marked
 //     hyperedge = all pairs (marked centre) or all pairs minus the pairs of
@@ -14,6 +15,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "hm_classes.h"
@@ -29,6 +33,7 @@ constexpr unsigned kWarps = kBlock / kWarp;
 constexpr unsigned kSlots = 8192;
 constexpr unsigned kRowMax = kSlots / 2;
 constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr unsigned kUnroll = 4;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ uint64_t global_warp() { return ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
@@ -73,15 +78,25 @@ __global__ void __launch_bounds__(kBlock) k_touch_open(const uint32_t* centres, 
       for (int t = 0; t < 4; ++t) hist[w][t][k] = 0;
     __syncwarp();
     const uint64_t base = off[a];
+    uint32_t one[4] = {0, 0, 0, 0};  // overlap-1 neighbours, the common case, counted in registers
     for (uint32_t k = lane; k < l; k += kWarp) {
       const uint32_t b = nbr[base + k];
       const uint32_t c = ovl[base + k];
       const uint32_t y = c < esize[b];
-      atomicAdd(&hist[w][y][c], 1u);
-      if (!ma && !mark[b]) atomicAdd(&hist[w][2 + y][c], 1u);
+      const bool um = !ma && !mark[b];
+      if (c == 1) {
+        one[y] += 1;
+        if (um) one[2 + y] += 1;
+      } else {
+        atomicAdd(&hist[w][y][c], 1u);
+        if (um) atomicAdd(&hist[w][2 + y][c], 1u);
+      }
     }
+    for (int t = 0; t < 4; ++t)
+      for (int d = 16; d; d >>= 1) one[t] += __shfl_xor_sync(0xffffffffu, one[t], d);
     __syncwarp();
     if (lane == 0) {
+      for (int t = 0; t < 4; ++t) hist[w][t][1] += one[t];
       for (int t = 0; t < 4; ++t)
         for (uint32_t k = 1; k <= s; ++k) hist[w][t][k] += hist[w][t][k - 1];
       open_pair_counts(hist[w][0], hist[w][1], s, acc, false);
@@ -131,6 +146,25 @@ struct TouchArgs {
   unsigned long long* out;  // 30 closed classes, 6 open-pair removals
 };
 
+__device__ __forceinline__ uint32_t size_cat(uint32_t s) { return s >= 3 ? 2u : s - 1u; }
+
+// Adds n triangles {m, b, c} whose three pairs share one node, the same one,
+// with size categories cm, cb, cc: closed class = number of members with
+// |x| >= 2; open-pair classes at each centre x: [|x| >= 3] + 2 ([|y| >= 2] +
+// [|z| >= 2]).
+__device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t cm, uint32_t cb, uint32_t cc, uint64_t n) {
+  const uint32_t em = cm > 0, eb = cb > 0, ec = cc > 0;
+  atomicAdd(&wc[em + eb + ec], (unsigned long long)n);
+  atomicAdd(&wc[30 + (cm == 2) + 2 * (eb + ec)], (unsigned long long)n);
+  atomicAdd(&wc[30 + (cb == 2) + 2 * (em + ec)], (unsigned long long)n);
+  atomicAdd(&wc[30 + (cc == 2) + 2 * (em + eb)], (unsigned long long)n);
+}
+
+// One block per marked m: row(m) in a bucketized shared-memory hash (4 keys
+// per 16-byte bucket), warps over b in row(m), lanes over the neighbours
+// c > b of b, four probes in flight per lane. A triangle {m, b, c} is counted
+// at its smallest marked id. Star triangles (all overlaps 1, one shared
+// node) are counted per size category in registers.
 __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
   extern __shared__ uint64_t smem64[];
   uint64_t* smask = smem64;
@@ -151,86 +185,137 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     const uint32_t md = A.len[m];
     const uint32_t sm = A.esize[m];
     const bool in_smem = md <= kRowMax;
-    uint32_t shift = 32, hmask = 0;
+    uint32_t shift = 32, bmask = 0;
     if (in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * md && slots < kSlots) slots <<= 1;
-      shift = 32 - (31 - __clz(slots));
-      hmask = slots - 1;
+      const uint32_t buckets = slots / 4;
+      shift = 32 - (31 - __clz(buckets));
+      bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
       for (uint32_t i = threadIdx.x; i < md; i += blockDim.x) {
         const uint32_t key = A.nbr[mo + i];
-        uint32_t h = (key * 2654435761u) >> shift;
-        while (atomicCAS(&keys[h], kEmpty, key) != kEmpty) h = (h + 1) & hmask;
+        uint32_t bk = (key * 2654435761u) >> shift, h = 0;
+        for (bool done = false; !done; bk = (bk + 1) & bmask)
+          for (uint32_t t = 0; t < 4; ++t)
+            if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
+              h = 4 * bk + t;
+              done = true;
+              break;
+            }
         smask[h] = A.mask[mo + i];
         sovl[h] = A.ovl[mo + i];
       }
     }
     __syncthreads();
+    const uint32_t cat_m = size_cat(sm);
+    const bool exact = sm <= 64;
     for (uint32_t bi = w; bi < md; bi += kWarps) {
       const uint32_t b = A.nbr[mo + bi];
+      if (A.mark[b] && b < m) continue;  // counted at b
       const uint32_t cmb = A.ovl[mo + bi];
       const uint64_t mmb = A.mask[mo + bi];
       const uint32_t sb = A.esize[b];
-      const bool mark_b_before = A.mark[b] && b < m;
-      if (mark_b_before) continue;  // counted at b
       const uint64_t bo = A.off[b];
       const uint32_t bl = A.len[b];
-      // first neighbour of b with an id above b
-      uint32_t lo = 0, hi = bl;
+      uint32_t lo = 0, hi = bl;  // first neighbour of b above b
       while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         if (A.nbr[bo + mid] <= b) lo = mid + 1;
         else hi = mid;
       }
-      for (uint32_t j = lo + lane; j < bl; j += kWarp) {
-        const uint32_t c = A.nbr[bo + j];
-        uint32_t cmc = 0;
-        uint64_t mmc = 0;
-        if (in_smem) {
-          uint32_t h = (c * 2654435761u) >> shift;
-          uint32_t k = keys[h];
-          while (k != c && k != kEmpty) {
-            h = (h + 1) & hmask;
-            k = keys[h];
-          }
-          if (k == c) {
-            cmc = sovl[h];
-            mmc = smask[h];
-          }
-        } else {
-          uint32_t l2 = 0, h2 = md;
-          while (l2 < h2) {
-            const uint32_t mid = (l2 + h2) >> 1;
-            if (A.nbr[mo + mid] < c) l2 = mid + 1;
-            else h2 = mid;
-          }
-          if (l2 < md && A.nbr[mo + l2] == c) {
-            cmc = A.ovl[mo + l2];
-            mmc = A.mask[mo + l2];
+      uint32_t star0 = 0, star1 = 0, star2 = 0;
+      for (uint32_t j0 = lo; j0 < bl; j0 += kWarp * kUnroll) {
+        uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+        for (unsigned u = 0; u < kUnroll; ++u) {
+          const uint32_t j = j0 + u * kWarp + lane;
+          cv[u] = kEmpty;
+          ov[u] = 0;
+          if (j < bl) {
+            cv[u] = __ldg(A.nbr + bo + j);
+            ov[u] = __ldg(A.ovl + bo + j);
           }
         }
-        if (!cmc) continue;
-        if (A.mark[c] && c < m) continue;  // counted at c
-        const uint32_t cbc = A.ovl[bo + j];
-        const uint32_t sc = A.esize[c];
-        const uint32_t g = sm <= 64 ? (uint32_t)__popcll(mmb & mmc) : triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
-        const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
-        if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-        const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
-        const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
-        const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
-        const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
-        const unsigned peers = __match_any_sync(__activemask(), key);
-        if (lane == (unsigned)(__ffs(peers) - 1)) {
-          const unsigned long long cnt = (unsigned long long)__popc(peers);
-          atomicAdd(&wc[k], cnt);
-          atomicAdd(&wc[30 + om], cnt);
-          atomicAdd(&wc[30 + ob], cnt);
-          atomicAdd(&wc[30 + oc], cnt);
+#pragma unroll
+        for (unsigned u = 0; u < kUnroll; ++u) {
+          const uint32_t c = cv[u];
+          if (c == kEmpty) continue;
+          uint32_t cmc = 0;
+          uint64_t mmc = 0;
+          if (in_smem) {
+            uint32_t bk = (c * 2654435761u) >> shift;
+            int t;
+            for (;;) {
+              const uint4 q = reinterpret_cast<const uint4*>(keys)[bk];
+              t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
+              if (t >= 0 || q.w == kEmpty) break;
+              bk = (bk + 1) & bmask;
+            }
+            if (t >= 0) {
+              cmc = sovl[4 * bk + t];
+              mmc = smask[4 * bk + t];
+            }
+          } else {
+            uint32_t l2 = 0, h2 = md;
+            while (l2 < h2) {
+              const uint32_t mid = (l2 + h2) >> 1;
+              if (A.nbr[mo + mid] < c) l2 = mid + 1;
+              else h2 = mid;
+            }
+            if (l2 < md && A.nbr[mo + l2] == c) {
+              cmc = A.ovl[mo + l2];
+              mmc = A.mask[mo + l2];
+            }
+          }
+          if (!cmc) continue;
+          if (A.mark[c] && c < m) continue;  // counted at c
+          const uint32_t cbc = ov[u];
+          const uint32_t sc = A.esize[c];
+          uint32_t g;
+          if (exact) {
+            if ((cmb | cmc | cbc) == 1 && mmb == mmc) {
+              const uint32_t cc = size_cat(sc);
+              star0 += cc == 0;
+              star1 += cc == 1;
+              star2 += cc == 2;
+              continue;
+            }
+            g = (uint32_t)__popcll(mmb & mmc);
+          } else {
+            g = triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
+          }
+          const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
+          if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+          const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
+          const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
+          const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
+          const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
+          const unsigned peers = __match_any_sync(__activemask(), key);
+          if (lane == (unsigned)(__ffs(peers) - 1)) {
+            const unsigned long long cnt = (unsigned long long)__popc(peers);
+            atomicAdd(&wc[k], cnt);
+            atomicAdd(&wc[30 + om], cnt);
+            atomicAdd(&wc[30 + ob], cnt);
+            atomicAdd(&wc[30 + oc], cnt);
+          }
         }
       }
+      if (cmb == 1 && exact) {
+        for (int d = 16; d; d >>= 1) {
+          star0 += __shfl_xor_sync(0xffffffffu, star0, d);
+          star1 += __shfl_xor_sync(0xffffffffu, star1, d);
+          star2 += __shfl_xor_sync(0xffffffffu, star2, d);
+        }
+        if (lane == 0) {
+          const uint32_t cat_b = size_cat(sb);
+          if (star0) add_star(wc, cat_m, cat_b, 0, star0);
+          if (star1) add_star(wc, cat_m, cat_b, 1, star1);
+          if (star2) add_star(wc, cat_m, cat_b, 2, star2);
+        }
+      }
+      __syncwarp();
     }
     __syncthreads();
   }
@@ -272,6 +357,8 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
   HM_TRY(centres.alloc(ctx, nc));
   k_list_flagged<<<grid_for(E, kBlock), kBlock, 0, st>>>(flag.p, pos.p, E, centres.p);
   HM_LAUNCH_CHECK();
+  const bool trace = std::getenv("HM_TRACE") != nullptr;
+  auto t_open0 = std::chrono::steady_clock::now();
   k_touch_open<<<grid_for(nc * 32, kBlock), kBlock, 0, st>>>(centres.p, (uint32_t)nc, mark.p, g->h2h_off.p,
                                                              g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->esize.p,
                                                              cnt.p + 36);
@@ -283,8 +370,17 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
   }
   TouchArgs A{d_ids, n, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
               g->h2v_off.p, g->h2v_mem.p, g->esize.p, reinterpret_cast<unsigned int*>(cnt.p + 42), cnt.p};
+  if (trace) cudaStreamSynchronize(st);
+  auto t_cl0 = std::chrono::steady_clock::now();
   k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n), kBlock, touch_smem(), st>>>(A);
   HM_LAUNCH_CHECK();
+  if (trace) {
+    cudaStreamSynchronize(st);
+    const auto t_end = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[hm_trace touching] marked=%u centres=%llu open=%.1fms closed=%.1fms\n", n,
+                 (unsigned long long)nc, std::chrono::duration<double, std::milli>(t_cl0 - t_open0).count(),
+                 std::chrono::duration<double, std::milli>(t_end - t_cl0).count());
+  }
   unsigned long long h[44];
   HM_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));

@@ -42,8 +42,9 @@ constexpr unsigned kClosedWarps = kClosedBlock / kWarp;
 constexpr unsigned kUnroll = 4;               // probes in flight per lane
 constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair classes
 // Two launch shapes of the closed phase: rows up to kSmallRow with a 4096-slot
-// table (4 blocks per SM), longer rows with an 8192-slot table (2 per SM).
-constexpr unsigned kSmallRow = 1024;
+// bucketized table (4 blocks per SM, load <= 1/2), longer rows with an
+// 8192-slot table (2 per SM).
+constexpr unsigned kSmallRow = 2048;
 constexpr uint32_t kEmpty = 0xffffffffu;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -180,6 +181,7 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
 // counter updates aggregated across the lanes that share them.
 template <unsigned kHashSlotsMax, unsigned kMinBlocks>
 __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
+  static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
   constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
   extern __shared__ uint64_t smem64[];
   uint64_t* smask = smem64;                                            // kHashSlotsMax
@@ -202,18 +204,28 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t sa = A.esize[a];
     const bool in_smem = ad <= kHashRowMax;
     const bool flags = A.edge_flags != nullptr;
-    uint32_t shift = 32, mask = 0;
+    // Bucketized table: 4 keys per 16-byte bucket, filled in order, so one
+    // vector load answers a lookup unless the bucket is full (rare at load
+    // factors <= 1/2).
+    uint32_t shift = 32, bmask = 0;
     if (in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
-      shift = 32 - (31 - __clz(slots));
-      mask = slots - 1;
+      const uint32_t buckets = slots / 4;
+      shift = 32 - (31 - __clz(buckets));
+      bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
       for (uint32_t i = threadIdx.x; i < ad; i += blockDim.x) {
         const uint32_t key = A.pnbr[ao + i];
-        uint32_t h = hash_slot(key, shift);
-        while (atomicCAS(&keys[h], kEmpty, key) != kEmpty) h = (h + 1) & mask;
+        uint32_t bk = hash_slot(key, shift), h = 0;
+        for (bool done = false; !done; bk = (bk + 1) & bmask)
+          for (uint32_t t = 0; t < 4; ++t)
+            if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
+              h = 4 * bk + t;
+              done = true;
+              break;
+            }
         smask[h] = flags ? (uint64_t)i : A.pmask[ao + i];  // diagnostics keep the row index
         sovl[h] = (uint8_t)(A.pos[ao + i] & 0xffu);
       }
@@ -250,13 +262,16 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
           uint32_t cac = 0;
           uint64_t mac = 0;
           if (in_smem) {
-            uint32_t h = hash_slot(c, shift);
-            uint32_t k = keys[h];
-            while (k != c && k != kEmpty) {
-              h = (h + 1) & mask;
-              k = keys[h];
+            uint32_t bk = hash_slot(c, shift);
+            int t;
+            for (;;) {
+              const uint4 q = reinterpret_cast<const uint4*>(keys)[bk];
+              t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
+              if (t >= 0 || q.w == kEmpty) break;
+              bk = (bk + 1) & bmask;
             }
-            if (k == c) {
+            if (t >= 0) {
+              const uint32_t h = 4 * bk + (uint32_t)t;
               cac = sovl[h];
               mac = smask[h];
               if (flags) {

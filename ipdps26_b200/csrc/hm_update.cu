@@ -25,6 +25,10 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "hm_classes.h"
@@ -348,6 +352,41 @@ __global__ void k_compact_members(const uint64_t* off, const uint32_t* len, uint
   }
 }
 
+__global__ void k_arena_keys(const uint64_t* off, uint32_t n, uint64_t* key, uint32_t* slot) {
+  for (uint64_t r = gtid(); r < n; r += gstride()) {
+    key[r] = off[r];
+    slot[r] = (uint32_t)r;
+  }
+}
+
+// phase 0: rows -> staging buffer (positions relative to base);
+// phase 1: staging -> final position, and the row offset is updated.
+__global__ void k_stage_rows(const uint32_t* slots, uint32_t n, uint64_t* off, const uint32_t* len,
+                             const uint64_t* dst, uint64_t base, uint32_t* nbr, uint8_t* ovl, uint64_t* mask,
+                             uint32_t* snbr, uint8_t* sovl, uint64_t* smask, int phase) {
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t r = slots[i];
+    const uint32_t l = len[r];
+    const uint64_t t = dst[i] - base;
+    if (phase == 0) {
+      const uint64_t s = off[r];
+      for (uint32_t k = lane_id(); k < l; k += kWarp) {
+        snbr[t + k] = nbr[s + k];
+        sovl[t + k] = ovl[s + k];
+        smask[t + k] = mask[s + k];
+      }
+    } else {
+      const uint64_t d = dst[i];
+      for (uint32_t k = lane_id(); k < l; k += kWarp) {
+        nbr[d + k] = snbr[t + k];
+        ovl[d + k] = sovl[t + k];
+        mask[d + k] = smask[t + k];
+      }
+      if (lane_id() == 0) off[r] = d;
+    }
+  }
+}
+
 __global__ void k_set_off(const uint64_t* new_off, uint32_t n, uint64_t* off) {
   for (uint64_t r = gtid(); r < n; r += gstride()) off[r] = new_off[r];
 }
@@ -388,7 +427,73 @@ static int ensure_slots(hm_graph* g, uint32_t need) {
 
 // Re-packs the H2H arena so that the live rows are contiguous, leaving room
 // for extra more entries.
-static int compact_h2h(hm_graph* g, uint64_t extra) {
+// Moves the live H2H rows to the front of the arena, in place: rows are
+// taken in arena order and moved in rounds through a bounded staging buffer;
+// each row only moves towards the front, and every round reads its rows
+// before writing them, so no row is overwritten before it is read.
+static int compact_h2h_in_place(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  if (!E) {
+    g->h2h_tail = 0;
+    return HM_OK;
+  }
+  // slots in arena order (empty rows sort anywhere; they move nothing)
+  DArr<uint64_t> key, key_s;
+  DArr<uint32_t> slot, slot_s, len_s;
+  HM_TRY(key.alloc(ctx, E));
+  HM_TRY(key_s.alloc(ctx, E));
+  HM_TRY(slot.alloc(ctx, E));
+  HM_TRY(slot_s.alloc(ctx, E));
+  HM_TRY(len_s.alloc(ctx, E));
+  k_arena_keys<<<grid_for(E, kBlock), kBlock, 0, st>>>(g->h2h_off.p, E, key.p, slot.p);
+  HM_LAUNCH_CHECK();
+  {
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, key_s.p, slot.p, slot_s.p, (int64_t)E, 0, 64, st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, key_s.p, slot.p, slot_s.p, (int64_t)E, 0, 64, st));
+  }
+  k_gather_u32<<<grid_for(E, kBlock), kBlock, 0, st>>>(slot_s.p, E, g->h2h_len.p, len_s.p);
+  HM_LAUNCH_CHECK();
+  DArr<uint64_t> noff;
+  HM_TRY(noff.alloc(ctx, (size_t)E + 1));
+  HM_TRY(exclusive_scan(ctx, len_s.p, noff.p, E));
+  std::vector<uint64_t> h((size_t)E + 1);
+  HM_CUDA(cudaMemcpyAsync(h.data(), noff.p, sizeof(uint64_t) * ((size_t)E + 1), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  const uint64_t live = h[E];
+  uint64_t stage_cap = std::min<uint64_t>(std::max<uint64_t>(live, 1), 1ull << 28);
+  uint64_t max_row = 0;
+  for (uint32_t r = 0; r < E; ++r) max_row = std::max(max_row, h[r + 1] - h[r]);
+  stage_cap = std::max(stage_cap, max_row);
+  DArr<uint32_t> snbr;
+  DArr<uint8_t> sovl;
+  DArr<uint64_t> smask;
+  HM_TRY(snbr.alloc(ctx, stage_cap));
+  HM_TRY(sovl.alloc(ctx, stage_cap));
+  HM_TRY(smask.alloc(ctx, stage_cap));
+  uint32_t r0 = 0;
+  while (r0 < E) {
+    uint32_t r1 = r0;
+    while (r1 < E && h[r1 + 1] - h[r0] <= stage_cap) ++r1;
+    const uint32_t n = r1 - r0;
+    for (int phase = 0; phase < 2; ++phase) {
+      k_stage_rows<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(
+          slot_s.p + r0, n, g->h2h_off.p, g->h2h_len.p, noff.p + r0, h[r0], g->h2h_nbr.p, g->h2h_ovl.p,
+          g->h2h_mask.p, snbr.p, sovl.p, smask.p, phase);
+      HM_LAUNCH_CHECK();
+    }
+    r0 = r1;
+  }
+  g->h2h_tail = live;
+  return HM_OK;
+}
+
+// Replaces the arena by one of cap entries holding the live rows compactly.
+static int regrow_h2h(hm_graph* g, uint64_t cap) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const uint32_t E = g->n_slots;
@@ -398,15 +503,10 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   uint64_t live = 0;
   HM_CUDA(cudaMemcpyAsync(&live, noff.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
-  const uint64_t cap = live + extra + (live + extra) / 4 + 1024;
+  cap = std::max<uint64_t>(cap, live + 1024);
   DArr<uint32_t> nnbr;
   DArr<uint8_t> novl;
   DArr<uint64_t> nmask;
-  // the oriented copy is rebuilt on demand; drop it first to make room
-  g->plus_nbr.release();
-  g->plus_os.release();
-  g->plus_mask.release();
-  g->plus_valid = false;
   HM_TRY(nnbr.alloc(ctx, cap));
   HM_TRY(novl.alloc(ctx, cap));
   HM_TRY(nmask.alloc(ctx, cap));
@@ -424,6 +524,21 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   g->h2h_cap = cap;
   g->h2h_tail = live;
   return HM_OK;
+}
+
+// The arena keeps room for rewriting about as many entries as are live: a
+// batch on a hub-heavy graph rewrites most rows. It is grown once (to twice
+// the live entries, dropping the oriented copy, which is rebuilt on demand),
+// then compacted in place whenever the tail runs out.
+static int compact_h2h(hm_graph* g, uint64_t extra) {
+  g->plus_nbr.release();
+  g->plus_os.release();
+  g->plus_mask.release();
+  g->plus_valid = false;
+  HM_TRY(compact_h2h_in_place(g));
+  if (g->h2h_tail + extra <= g->h2h_cap) return HM_OK;
+  const uint64_t live = g->h2h_tail;
+  return regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
 }
 
 // Room for n more entries at the H2H arena tail; returns the position.
@@ -460,6 +575,33 @@ static int compact_h2v(hm_graph* g, uint64_t extra) {
 }
 
 int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]);
+
+// Per-phase wall times of one batch, printed to stderr when HM_TRACE is set
+// in the environment (each mark synchronises the stream; diagnostics only).
+struct PhaseTrace {
+  cudaStream_t st;
+  bool on;
+  std::chrono::steady_clock::time_point t0;
+  std::string out;
+  explicit PhaseTrace(cudaStream_t s) : st(s), on(std::getenv("HM_TRACE") != nullptr) {
+    if (on) {
+      cudaStreamSynchronize(st);
+      t0 = std::chrono::steady_clock::now();
+    }
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const auto t = std::chrono::steady_clock::now();
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), " %s=%.1fms", name, std::chrono::duration<double, std::milli>(t - t0).count());
+    out += buf;
+    t0 = t;
+  }
+  ~PhaseTrace() {
+    if (on) std::fprintf(stderr, "[hm_trace apply_batch]%s\n", out.c_str());
+  }
+};
 
 // Deletes, inserts, and optionally reports the exact change of the 30 static
 // classes. All device work; the host only sequences the kernels.
@@ -505,12 +647,15 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
   static const uint64_t zero_off = 0;
   HM_TRY(build_h2v(&ins, n_ins ? h_ins_off : &zero_off, h_ins_mem, n_ins));
 
+  PhaseTrace trace(st);
+  trace.mark("validate");
   int64_t before[30] = {0};
   if (delta30 && n_del) {
     uint64_t c[30];
     HM_TRY(count_touching(g, dels.p, n_del, c));
     for (int k = 0; k < 30; ++k) before[k] = (int64_t)c[k];
   }
+  trace.mark("count_deleted");
 
   // ---- deletions: H2H removal patches from the rows about to vanish ----------
   DArr<uint64_t> rem_off;
@@ -587,8 +732,10 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
   g->h2v_nnz = g->h2v_nnz + ins_members;  // deleted members are subtracted below
   g->n_live = g->n_live - n_del + n_ins;
 
+  trace.mark("delete_assign_h2v");
   // ---- V2H from the live rows -----------------------------------------------------
   HM_TRY(build_v2h(g));
+  trace.mark("v2h");
 
   // ---- H2H: fresh rows for the inserted ids -------------------------------------
   DArr<uint8_t> ins_mark, skip;
@@ -611,6 +758,7 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
     HM_TRY(h2h_rows_for(g, ids.p, n_ins, reserve, &written));
   }
 
+  trace.mark("h2h_inserted_rows");
   // ---- H2H addition patches ---------------------------------------------------
   DArr<uint32_t> ilen;
   DArr<uint64_t> ioff;
@@ -738,6 +886,7 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
     }
   }
 
+  trace.mark("h2h_patch");
   // ---- bookkeeping ---------------------------------------------------------------
   DArr<unsigned long long> sums;
   HM_TRY(sums.alloc(ctx, 2));
@@ -754,9 +903,11 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
   g->plus_valid = false;
   g->work_valid = false;
 
+  trace.mark("bookkeeping");
   if (delta30) {
     uint64_t c[30] = {0};
     if (n_ins) HM_TRY(count_touching(g, ids.p, n_ins, c));
+    trace.mark("count_inserted");
     for (int k = 0; k < 30; ++k) delta30[k] = (int64_t)c[k] - before[k];
   }
   HM_CUDA(cudaEventRecord(e1, st));

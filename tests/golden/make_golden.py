@@ -82,11 +82,52 @@ def temporal_graph(c):
     return gen.temporal(gen.params(dedupe=dedupe, **kw), **c["burst"])
 
 
+FULL_CASES = {
+    # config 1 exactly as specified (MoCHy main_exact_par on all host cores)
+    "config1-full": dict(kind="static", params=dict(seed=0, n_nodes=10000, n_edges=20000, k_min=2, k_max=25,
+                                                    size_exp=2.5, pop_exp=1.2, pop_offset=0.0)),
+    # config 4 as specified (THyMe+ main_thymeP on all host cores), smallest window
+    "config4-full-d1000": dict(kind="temporal", params=dict(
+        gen=dict(seed=3, n_nodes=200000, n_edges=500000, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2,
+                 pop_offset=0.0, dedupe=False),
+        burst=dict(burst_rate=1e-4, events_per_burst=50, gap_mean=20.0, span=100_000_000), deltas=[1000])),
+}
+
+
+def run_full(names, threads, timeout):
+    """Full-size cases: parallel reference programs only (hours of CPU)."""
+    fp = OUT / "full_golden.json"
+    for name in names:
+        c = FULL_CASES[name]
+        if c["kind"] == "static":
+            h = static_graph(c["params"])
+            counts, wall, _ = rr.run_mochy(h.offsets, h.members, threads=threads, timeout=timeout)
+            rec = dict(kind="static", params=c["params"], sha256=digest(h), n_edges=h.n_edges,
+                       counts26=counts.tolist(), mochy_par_wall_s=round(wall, 1), threads=threads)
+        else:
+            h = temporal_graph(c["params"])
+            rec = dict(kind="temporal", params=c["params"], sha256=digest(h), n_events=h.n_edges, counts96={},
+                       threads=threads)
+            for d in c["params"]["deltas"]:
+                x, wall, _ = rr.run_thyme(h.offsets, h.members, h.timestamps, d, threads=threads, timeout=timeout)
+                rec["counts96"][str(d)] = x.tolist()
+                rec[f"thymeP_wall_s_{d}"] = round(wall, 1)
+        print(name, "done", flush=True)
+        merged = json.loads(fp.read_text()) if fp.exists() else {}  # other runs may have written meanwhile
+        merged[name] = rec
+        fp.write_text(json.dumps(merged, indent=1))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--timeout", type=float, default=900)
+    ap.add_argument("--full", nargs="*", help="run these full-size cases instead")
+    ap.add_argument("--threads", type=int, default=8)
     a = ap.parse_args()
+    if a.full is not None:
+        run_full(a.full or list(FULL_CASES), a.threads, a.timeout)
+        return
     sp = OUT / "static_golden.json"
     tp = OUT / "temporal_golden.json"
     sg = json.loads(sp.read_text()) if sp.exists() else {}
