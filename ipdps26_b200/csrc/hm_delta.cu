@@ -10,8 +10,8 @@
 //     hyperedge = all pairs (marked centre) or all pairs minus the pairs of
 //     unmarked neighbours (unmarked centre), counted from histograms;
 //   * closed phase, one block per marked m: row(m) in a shared-memory hash;
-//     each warp takes b in row(m), its lanes walk the neighbours c > b of b
-//     and probe. A triangle {m, b, c} is counted at its smallest marked id.
+//     each warp takes b in row(m), its lanes walk the oriented row N+(b) and
+//     probe. A triangle {m, b, c} is counted at its smallest marked id.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -30,8 +30,8 @@ namespace {
 constexpr unsigned kWarp = 32;
 constexpr unsigned kBlock = 256;
 constexpr unsigned kWarps = kBlock / kWarp;
-constexpr unsigned kSlots = 8192;
-constexpr unsigned kRowMax = kSlots / 2;
+constexpr unsigned kSlots = 16384;        // shared table of one marked row
+constexpr unsigned kRowMax = kSlots / 2;  // longer rows use a global table
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr unsigned kUnroll = 4;
 
@@ -142,6 +142,15 @@ struct TouchArgs {
   const uint64_t* hoff;
   const uint32_t* hmem;
   const uint8_t* esize;
+  const uint64_t* poff;     // oriented rows: neighbours of higher (degree, id) rank
+  const uint32_t* plen;
+  const uint32_t* pnbr;
+  const uint16_t* pos;      // (neighbour size << 8) | overlap
+  const uint64_t* pmask;    // shared positions of the row owner's members
+  const uint64_t* goff;     // per item: offset of its global table (rows longer than kRowMax)
+  const uint32_t* gslots;   // per item: slots of that table, 0 for a shared-memory row
+  const uint32_t* brange;   // per item: [brange[2i], brange[2i+1]) of row(m) to take b from
+  const unsigned long long* gtab;
   unsigned int* queue;
   unsigned long long* out;  // 30 closed classes, 6 open-pair removals
 };
@@ -160,16 +169,41 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t cm, ui
   atomicAdd(&wc[30 + (cc == 2) + 2 * (em + eb)], (unsigned long long)n);
 }
 
-// One block per marked m: row(m) in a bucketized shared-memory hash (4 keys
-// per 16-byte bucket), warps over b in row(m), lanes over the neighbours
-// c > b of b, four probes in flight per lane. A triangle {m, b, c} is counted
-// at its smallest marked id. Star triangles (all overlaps 1, one shared
-// node) are counted per size category in registers.
+__device__ __forceinline__ uint32_t hmix(uint32_t key) { return key * 2654435761u; }
+
+// Global-memory tables of the marked rows too long for shared memory: entry
+// (neighbour << 32) | index in the row, all ones when empty.
+__global__ void k_build_ghash(const uint32_t* ids, uint32_t n, const uint64_t* goff, const uint32_t* gslots,
+                              const uint32_t* brange, const uint64_t* off, const uint32_t* len, const uint32_t* nbr,
+                              unsigned long long* tab) {
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t slots = gslots[i];
+    if (!slots || brange[2 * i] != 0) continue;  // one build per row: its first slice
+    const uint32_t m = ids[i];
+    unsigned long long* t = tab + goff[i];
+    const uint64_t mo = off[m];
+    for (uint32_t k = lane_id(); k < len[m]; k += kWarp) {
+      const uint32_t key = nbr[mo + k];
+      const unsigned long long e = ((unsigned long long)key << 32) | k;
+      uint32_t h = hmix(key) & (slots - 1);
+      while (atomicCAS(&t[h], ~0ull, e) != ~0ull) h = (h + 1) & (slots - 1);
+    }
+  }
+}
+
+// One block per marked m, heaviest rows first: row(m) in a bucketized
+// shared-memory table (4 keys per 16-byte bucket, with the row index of each
+// key) or, for rows longer than kRowMax, in a global table; warps take b in
+// row(m), lanes walk N+(b), the neighbours of b ranked above b by (degree,
+// id), with four probes in flight. A
+// triangle {m, b, c} is counted at its smallest marked id. g comes from the
+// position masks of m (|m| <= 64) or of b (|b| <= 64), else from a merge.
+// Star triangles (all overlaps 1, one shared node) are counted per size
+// category in registers.
 __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
-  extern __shared__ uint64_t smem64[];
-  uint64_t* smask = smem64;
-  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kSlots);
-  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kSlots);
+  extern __shared__ uint32_t smem32[];
+  uint32_t* keys = smem32;                                         // kSlots
+  uint16_t* sidx = reinterpret_cast<uint16_t*>(keys + kSlots);     // kSlots
   __shared__ unsigned long long wcnt[kWarps][36];
   __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
@@ -184,11 +218,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     const uint64_t mo = A.off[m];
     const uint32_t md = A.len[m];
     const uint32_t sm = A.esize[m];
-    const bool in_smem = md <= kRowMax;
+    const uint32_t gslots = A.gslots[item];
+    const unsigned long long* gt = A.gtab + A.goff[item];
     uint32_t shift = 32, bmask = 0;
-    if (in_smem) {
+    if (!gslots) {
       uint32_t slots = 64;
-      while (slots < 4 * md && slots < kSlots) slots <<= 1;
+      while (slots < 2 * md && slots < kSlots) slots <<= 1;
       const uint32_t buckets = slots / 4;
       shift = 32 - (31 - __clz(buckets));
       bmask = buckets - 1;
@@ -196,7 +231,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
       __syncthreads();
       for (uint32_t i = threadIdx.x; i < md; i += blockDim.x) {
         const uint32_t key = A.nbr[mo + i];
-        uint32_t bk = (key * 2654435761u) >> shift, h = 0;
+        uint32_t bk = hmix(key) >> shift, h = 0;
         for (bool done = false; !done; bk = (bk + 1) & bmask)
           for (uint32_t t = 0; t < 4; ++t)
             if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
@@ -204,27 +239,36 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
               done = true;
               break;
             }
-        smask[h] = A.mask[mo + i];
-        sovl[h] = A.ovl[mo + i];
+        sidx[h] = (uint16_t)i;
       }
     }
     __syncthreads();
     const uint32_t cat_m = size_cat(sm);
-    const bool exact = sm <= 64;
-    for (uint32_t bi = w; bi < md; bi += kWarps) {
+    const uint32_t b_begin = A.brange[2 * item], b_end = A.brange[2 * item + 1];
+    for (uint32_t bi = b_begin + w; bi < b_end; bi += kWarps) {
       const uint32_t b = A.nbr[mo + bi];
       if (A.mark[b] && b < m) continue;  // counted at b
       const uint32_t cmb = A.ovl[mo + bi];
-      const uint64_t mmb = A.mask[mo + bi];
       const uint32_t sb = A.esize[b];
-      const uint64_t bo = A.off[b];
-      const uint32_t bl = A.len[b];
-      uint32_t lo = 0, hi = bl;  // first neighbour of b above b
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (A.nbr[bo + mid] <= b) lo = mid + 1;
-        else hi = mid;
+      // c runs over N+(b), the neighbours of b ranked above it: each pair
+      // {b, c} of m's neighbours is met once, from its lower-ranked end
+      const uint64_t bo = A.poff[b];
+      const uint32_t bl = A.plen[b];
+      // masks: relative to m when |m| <= 64, else relative to b when |b| <= 64
+      const bool piv_m = sm <= 64, piv_b = !piv_m && sb <= 64;
+      uint64_t pmb = piv_m ? A.mask[mo + bi] : 0;
+      const uint32_t lo = 0;
+      if (piv_b) {  // b's entry for m, from b's full row
+        const uint64_t fo = A.off[b];
+        uint32_t l2 = 0, h2 = A.len[b];
+        while (l2 < h2) {
+          const uint32_t mid = (l2 + h2) >> 1;
+          if (A.nbr[fo + mid] < m) l2 = mid + 1;
+          else h2 = mid;
+        }
+        pmb = A.mask[fo + l2];
       }
+      const bool star_ok = cmb == 1 && (piv_m || piv_b);
       uint32_t star0 = 0, star1 = 0, star2 = 0;
       for (uint32_t j0 = lo; j0 < bl; j0 += kWarp * kUnroll) {
         uint32_t cv[kUnroll], ov[kUnroll];
@@ -234,18 +278,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
           cv[u] = kEmpty;
           ov[u] = 0;
           if (j < bl) {
-            cv[u] = __ldg(A.nbr + bo + j);
-            ov[u] = __ldg(A.ovl + bo + j);
+            cv[u] = __ldg(A.pnbr + bo + j);
+            ov[u] = __ldg(A.pos + bo + j);
           }
         }
 #pragma unroll
         for (unsigned u = 0; u < kUnroll; ++u) {
           const uint32_t c = cv[u];
           if (c == kEmpty) continue;
-          uint32_t cmc = 0;
-          uint64_t mmc = 0;
-          if (in_smem) {
-            uint32_t bk = (c * 2654435761u) >> shift;
+          int idx = -1;
+          if (!gslots) {
+            uint32_t bk = hmix(c) >> shift;
             int t;
             for (;;) {
               const uint4 q = reinterpret_cast<const uint4*>(keys)[bk];
@@ -253,36 +296,34 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
               if (t >= 0 || q.w == kEmpty) break;
               bk = (bk + 1) & bmask;
             }
-            if (t >= 0) {
-              cmc = sovl[4 * bk + t];
-              mmc = smask[4 * bk + t];
-            }
+            if (t >= 0) idx = sidx[4 * bk + t];
           } else {
-            uint32_t l2 = 0, h2 = md;
-            while (l2 < h2) {
-              const uint32_t mid = (l2 + h2) >> 1;
-              if (A.nbr[mo + mid] < c) l2 = mid + 1;
-              else h2 = mid;
-            }
-            if (l2 < md && A.nbr[mo + l2] == c) {
-              cmc = A.ovl[mo + l2];
-              mmc = A.mask[mo + l2];
+            uint32_t h = hmix(c) & (gslots - 1);
+            for (;;) {
+              const unsigned long long e = gt[h];
+              if (e == ~0ull) break;
+              if ((uint32_t)(e >> 32) == c) {
+                idx = (int)(uint32_t)e;
+                break;
+              }
+              h = (h + 1) & (gslots - 1);
             }
           }
-          if (!cmc) continue;
+          if (idx < 0) continue;
           if (A.mark[c] && c < m) continue;  // counted at c
-          const uint32_t cbc = ov[u];
-          const uint32_t sc = A.esize[c];
+          const uint32_t cmc = A.ovl[mo + idx];
+          const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
           uint32_t g;
-          if (exact) {
-            if ((cmb | cmc | cbc) == 1 && mmb == mmc) {
+          if (piv_m || piv_b) {
+            const uint64_t pmc = piv_m ? A.mask[mo + idx] : A.pmask[bo + j0 + u * kWarp + lane];
+            if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
               const uint32_t cc = size_cat(sc);
               star0 += cc == 0;
               star1 += cc == 1;
               star2 += cc == 2;
               continue;
             }
-            g = (uint32_t)__popcll(mmb & mmc);
+            g = (uint32_t)__popcll(pmb & pmc);
           } else {
             g = triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
           }
@@ -302,7 +343,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
           }
         }
       }
-      if (cmb == 1 && exact) {
+      if (star_ok) {
         for (int d = 16; d; d >>= 1) {
           star0 += __shfl_xor_sync(0xffffffffu, star0, d);
           star1 += __shfl_xor_sync(0xffffffffu, star1, d);
@@ -324,7 +365,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     if (wc[k]) atomicAdd(&A.out[k], wc[k]);
 }
 
-constexpr size_t touch_smem() { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * kSlots; }
+__global__ void k_gather_len(const uint32_t* ids, uint32_t n, const uint32_t* len, uint32_t* out) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) out[i] = len[ids[i]];
+}
+
+constexpr size_t touch_smem() { return (sizeof(uint32_t) + sizeof(uint16_t)) * kSlots; }
 
 }  // namespace
 
@@ -368,11 +413,72 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
     HM_CUDA(cudaFuncSetAttribute(k_touch_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)touch_smem()));
     attr = true;
   }
-  TouchArgs A{d_ids, n, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
-              g->h2v_off.p, g->h2v_mem.p, g->esize.p, reinterpret_cast<unsigned int*>(cnt.p + 42), cnt.p};
+  // heaviest rows first; rows longer than kRowMax get a global table
+  DArr<uint32_t> lens;
+  HM_TRY(lens.alloc(ctx, n));
+  k_gather_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, lens.p);
+  HM_LAUNCH_CHECK();
+  std::vector<uint32_t> hid(n), hlen(n), order(n);
+  HM_CUDA(cudaMemcpyAsync(hid.data(), d_ids, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaMemcpyAsync(hlen.data(), lens.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hlen[x] > hlen[y]; });
+  // items: one per marked row held in shared memory; rows in global tables
+  // are split into slices of kSlice neighbours b, one item each
+  constexpr uint32_t kSlice = 256;
+  std::vector<uint32_t> oid, oslots, orange;
+  std::vector<uint64_t> ooff;
+  uint64_t gtotal = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t id = hid[order[i]];
+    const uint32_t l = hlen[order[i]];
+    if (l > kRowMax) {
+      uint32_t sl = 1;
+      while (sl < 2 * l) sl <<= 1;
+      for (uint32_t b0 = 0; b0 < l; b0 += kSlice) {
+        oid.push_back(id);
+        oslots.push_back(sl);
+        ooff.push_back(gtotal);
+        orange.push_back(b0);
+        orange.push_back(std::min(l, b0 + kSlice));
+      }
+      gtotal += sl;
+    } else {
+      oid.push_back(id);
+      oslots.push_back(0);
+      ooff.push_back(0);
+      orange.push_back(0);
+      orange.push_back(l);
+    }
+  }
+  const uint32_t n_items = (uint32_t)oid.size();
+  DArr<uint32_t> d_oid, d_oslots, d_orange;
+  DArr<uint64_t> d_ooff;
+  DArr<unsigned long long> gtab;
+  HM_TRY(d_oid.alloc(ctx, n_items));
+  HM_TRY(d_oslots.alloc(ctx, n_items));
+  HM_TRY(d_orange.alloc(ctx, 2 * (size_t)n_items));
+  HM_TRY(d_ooff.alloc(ctx, n_items));
+  HM_TRY(gtab.alloc(ctx, gtotal ? gtotal : 1));
+  HM_CUDA(cudaMemcpyAsync(d_oid.p, oid.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, st));
+  HM_CUDA(cudaMemcpyAsync(d_oslots.p, oslots.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, st));
+  HM_CUDA(cudaMemcpyAsync(d_orange.p, orange.data(), sizeof(uint32_t) * 2 * n_items, cudaMemcpyHostToDevice, st));
+  HM_CUDA(cudaMemcpyAsync(d_ooff.p, ooff.data(), sizeof(uint64_t) * n_items, cudaMemcpyHostToDevice, st));
+  if (gtotal) {
+    HM_CUDA(cudaMemsetAsync(gtab.p, 0xff, sizeof(unsigned long long) * gtotal, st));
+    k_build_ghash<<<grid_for((uint64_t)n_items * 32, kBlock), kBlock, 0, st>>>(
+        d_oid.p, n_items, d_ooff.p, d_oslots.p, d_orange.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, gtab.p);
+    HM_LAUNCH_CHECK();
+  }
+  if (!g->plus_valid) HM_TRY(build_plus(g));
+  TouchArgs A{d_oid.p, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
+              g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
+              g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
+              reinterpret_cast<unsigned int*>(cnt.p + 42), cnt.p};
   if (trace) cudaStreamSynchronize(st);
   auto t_cl0 = std::chrono::steady_clock::now();
-  k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n), kBlock, touch_smem(), st>>>(A);
+  k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n_items), kBlock, touch_smem(), st>>>(A);
   HM_LAUNCH_CHECK();
   if (trace) {
     cudaStreamSynchronize(st);

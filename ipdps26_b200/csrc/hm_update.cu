@@ -536,8 +536,10 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   g->plus_mask.release();
   g->plus_valid = false;
   HM_TRY(compact_h2h_in_place(g));
-  if (g->h2h_tail + extra <= g->h2h_cap) return HM_OK;
   const uint64_t live = g->h2h_tail;
+  // keep at least half the live size free after a compaction, so that a
+  // batch needs few of them
+  if (live + std::max<uint64_t>(extra, live / 2) <= g->h2h_cap) return HM_OK;
   return regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
 }
 
@@ -875,14 +877,41 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
       HM_LAUNCH_CHECK();
       HM_TRY(exclusive_scan(ctx, remf.p, remx.p, n_kept));
       HM_TRY(exclusive_scan(ctx, addf.p, addx.p, n_kept));
-      uint64_t base = 0;
-      HM_TRY(reserve_h2h(g, need, &base));
-      k_patch_apply<<<grid_for(n_rows * 32, kBlock), kBlock, 0, st>>>(
-          rp.p, (uint32_t)n_rows, noff.p, base, pid.p, pop.p, ppidx.p, remx.p, addx.p, povl.p + n_rem,
-          pmask.p + n_rem, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
-      HM_LAUNCH_CHECK();
-      k_set_lens<<<grid_for(n_rows, kBlock), kBlock, 0, st>>>(rp.p, (uint32_t)n_rows, nlen.p, g->h2h_len.p);
-      HM_LAUNCH_CHECK();
+      (void)need;
+      // Patched rows go to the arena tail in chunks that fit the free space;
+      // between chunks the arena is compacted in place, so a batch never
+      // needs a second copy of the store.
+      std::vector<uint64_t> hno(n_rows + 1);
+      HM_CUDA(cudaMemcpyAsync(hno.data(), noff.p, sizeof(uint64_t) * (n_rows + 1), cudaMemcpyDeviceToHost, st));
+      HM_CUDA(cudaStreamSynchronize(st));
+      uint64_t r0 = 0;
+      while (r0 < n_rows) {
+        uint64_t free_space = g->h2h_cap - g->h2h_tail;
+        if (hno[r0 + 1] - hno[r0] > free_space || (free_space < (hno[n_rows] - hno[r0]) && free_space < g->h2h_cap / 4)) {
+          HM_TRY(compact_h2h(g, hno[r0 + 1] - hno[r0]));
+          free_space = g->h2h_cap - g->h2h_tail;
+        }
+        uint64_t r1 = r0 + 1;
+        {
+          uint64_t lo = r0 + 1, hi = n_rows;  // largest r1 with hno[r1] - hno[r0] <= free_space
+          while (lo < hi) {
+            const uint64_t mid = (lo + hi + 1) / 2;
+            if (hno[mid] - hno[r0] <= free_space) lo = mid;
+            else hi = mid - 1;
+          }
+          r1 = lo;
+        }
+        const uint32_t nr = (uint32_t)(r1 - r0);
+        const uint64_t base = g->h2h_tail - hno[r0];  // dst = base + noff[r], modulo 2^64
+        k_patch_apply<<<grid_for((uint64_t)nr * 32, kBlock), kBlock, 0, st>>>(
+            rp.p + r0, nr, noff.p + r0, base, pid.p, pop.p, ppidx.p, remx.p, addx.p, povl.p + n_rem,
+            pmask.p + n_rem, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p);
+        HM_LAUNCH_CHECK();
+        k_set_lens<<<grid_for(nr, kBlock), kBlock, 0, st>>>(rp.p + r0, nr, nlen.p + r0, g->h2h_len.p);
+        HM_LAUNCH_CHECK();
+        g->h2h_tail += hno[r1] - hno[r0];
+        r0 = r1;
+      }
     }
   }
 
