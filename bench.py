@@ -313,6 +313,7 @@ def engine_arm(args, rank, world, local_rank):
             open_ms.append(t.open_ms)
         e1.record(stream)
         torch.cuda.synchronize()
+        closed_tri = int(g.timings().closed_triangles)
         wall = time.perf_counter() - t0
         if world > 1:
             dist.barrier()
@@ -384,7 +385,7 @@ def engine_arm(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": config_of(args, world), "gpu_launches": 3 * args.steps,
-            "triples_per_step": triples, "closed_triangles_per_step": int(g.timings().closed_triangles),
+            "triples_per_step": triples, "closed_triangles_per_step": closed_tri,
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
                       "device_gb": info.device_bytes / 1e9},

@@ -51,3 +51,34 @@ def test_no_device_means_clean_error():
         assert e.status < 0
     else:
         raise AssertionError("context creation succeeded without a device")
+
+
+def test_cpp_shim_compiles_and_links(tmp_path):
+    """The reference-shaped C++ shim (include/hmotif_cbst.hpp) builds against
+    the library (linking only; nothing runs without a GPU)."""
+    import shutil
+    import subprocess
+
+    cxx = shutil.which("g++")
+    if cxx is None:
+        return
+    src = tmp_path / "use_shim.cpp"
+    src.write_text(
+        '#include "hmotif_cbst.hpp"\n'
+        "int main(int argc, char**) {\n"
+        "  if (argc < 99) return 0;  // link check only\n"
+        "  hm::Context ctx(0);\n"
+        "  hm::HypergraphStore s(ctx, \"H2V\");\n"
+        "  int starts[2] = {0, 4}; int flat[8] = {1, 2, 0, 0, 2, 3, 0, 0};\n"
+        "  s.construct(starts, 2, flat, 8, 4);\n"
+        "  auto c = hm::computeMotifCounts(s);\n"
+        "  std::vector<int64_t> d; s.update({1}, {1, 3}, {2}, &d);\n"
+        "  s.findAndPrint({1, 2});\n"
+        "  return (int)c[0];\n"
+        "}\n")
+    out = tmp_path / "use_shim"
+    r = subprocess.run([cxx, "-std=c++17", f"-I{ROOT / 'include'}", str(src), "-o", str(out),
+                        f"-L{ROOT / 'ipdps26_b200'}", "-lhmotif", f"-Wl,-rpath,{ROOT / 'ipdps26_b200'}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(out)]).returncode == 0
