@@ -272,7 +272,7 @@ def reference_arm(args, rank, world):
 def engine_arm(args, rank, world, local_rank):
     import torch
 
-    from ipdps26_b200 import engine
+    from ipdps26_b200 import engine, shard
 
     dist = None
     if world > 1:
@@ -290,9 +290,7 @@ def engine_arm(args, rank, world, local_rank):
     def step():
         part = g.count_static30_shard(rank, world)
         if world > 1:
-            t = torch.from_numpy(part.view(np.int64)).to(f"cuda:{local_rank}")
-            dist.all_reduce(t)
-            part = t.cpu().numpy().view(np.uint64)
+            part = shard.allreduce_counts(part, dist, f"cuda:{local_rank}")
         return part
 
     for _ in range(args.warmup):
@@ -319,9 +317,7 @@ def engine_arm(args, rank, world, local_rank):
             dist.barrier()
     dev_s = e0.elapsed_time(e1) / 1000.0
     if world > 1:
-        tt = torch.tensor([dev_s], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_s = float(tt.item())
+        dev_s = shard.max_over_ranks(dev_s, dist, f"cuda:{local_rank}")
     triples = int(counts.astype(np.uint64).sum())
     value = triples * args.steps / dev_s
 

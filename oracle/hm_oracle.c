@@ -255,8 +255,12 @@ static int build_projection(const csr_t* h, uint32_t n_nodes, adj_t* adj) {
 /* ------------------------------------------------------------------------ */
 /* MoCHy exact restated (MoCHy-master/main_exact.cpp:91-129).                 */
 /* ------------------------------------------------------------------------ */
-int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
-                 uint64_t out30[30]) {
+/* Counts the triples owned by centres a = shard (mod n_shards): open triples
+ * at their centre, closed ones at a = min, the owner rule main_exact_par
+ * splits its parallel counting loop over a by (main_exact_par.cpp:122-173). The shards
+ * of one n_shards partition all triples. */
+int hmo_static30_shard(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
+                       uint32_t shard, uint32_t n_shards, uint64_t out30[30]) {
   csr_t h;
   adj_t adj;
   memset(out30, 0, sizeof(uint64_t) * 30);
@@ -272,6 +276,7 @@ int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* memb
   uint64_t* mk_tag = (uint64_t*)malloc(sizeof(uint64_t) * (n_edges ? n_edges : 1));
   for (uint32_t e = 0; e < n_edges; ++e) mk_tag[e] = UINT64_MAX;
   for (uint32_t a = 0; a < n_edges; ++a) {
+    if (a % n_shards != shard) continue;
     const uint32_t* ma = h.mem + h.off[a];
     uint32_t sa = (uint32_t)(h.off[a + 1] - h.off[a]);
     for (uint64_t i = adj.off[a]; i < adj.off[a + 1]; ++i) {
@@ -314,6 +319,11 @@ int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* memb
   adj_free(&adj);
   csr_free(&h);
   return 0;
+}
+
+int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
+                 uint64_t out30[30]) {
+  return hmo_static30_shard(n_edges, offsets, members, n_nodes, 0, 1, out30);
 }
 
 /* The 26 reported motifs: classes other than 0, 1, 4, 6

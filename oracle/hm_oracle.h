@@ -20,6 +20,8 @@ int hmo_temporal_class(int s1, int s2, int s3, int c12, int c23, int c31, int g)
 
 int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
                  uint64_t out30[30]);
+int hmo_static30_shard(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
+                       uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
 void hmo_static26_from30(const uint64_t in30[30], uint64_t out26[26]);
 int hmo_static30_brute(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint64_t out30[30]);
 

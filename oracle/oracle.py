@@ -31,6 +31,7 @@ def lib():
         L = C.CDLL(str(LIB))
         u32p, u64p, i64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_int64)
         L.hmo_static30.argtypes = [C.c_uint32, u64p, u32p, C.c_uint32, u64p]
+        L.hmo_static30_shard.argtypes = [C.c_uint32, u64p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, u64p]
         L.hmo_static30_brute.argtypes = [C.c_uint32, u64p, u32p, u64p]
         L.hmo_temporal96.argtypes = [C.c_uint32, u64p, u32p, i64p, C.c_int64, u64p]
         L.hmo_temporal96_brute.argtypes = [C.c_uint32, u64p, u32p, i64p, C.c_int64, u64p]
@@ -67,6 +68,17 @@ def static30(offsets, members, n_nodes: int) -> np.ndarray:
     rc = lib().hmo_static30(len(off) - 1, _p(off, C.c_uint64), _p(mem, C.c_uint32), n_nodes, _p(out, C.c_uint64))
     if rc != 0:
         raise RuntimeError(f"hmo_static30 failed: {rc}")
+    return out
+
+
+def static30_shard(offsets, members, n_nodes: int, shard: int, n_shards: int) -> np.ndarray:
+    """Triples owned by centres a = shard (mod n_shards)."""
+    off, mem = _csr(offsets, members)
+    out = np.zeros(30, np.uint64)
+    rc = lib().hmo_static30_shard(len(off) - 1, _p(off, C.c_uint64), _p(mem, C.c_uint32), n_nodes, shard, n_shards,
+                                  _p(out, C.c_uint64))
+    if rc != 0:
+        raise RuntimeError(f"hmo_static30_shard failed: {rc}")
     return out
 
 
