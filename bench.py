@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--no-update-check", action="store_true",
                     help="skip the full recount that checks the summed deltas")
     ap.add_argument("--no-temporal", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-graphs", type=int, default=256)
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="offered requests per second (Poisson)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the replayed trace")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -235,6 +240,48 @@ def temporal_section(ctx):
     return res
 
 
+def serve_section(args, ctx):
+    """Config 5: resident graphs behind the request loop. One seeded trace of
+    Poisson arrivals (70 % update batches of 100-10,000 edits, 80/20
+    insert/delete, 30 % full counts) is replayed at its arrival times through
+    the per-request form (one store per graph, one call per request) and
+    through the batched form (pooled store, one round of launches serves the
+    oldest waiting request of every graph); every result of the two replays
+    must be identical. Latencies are submit-to-done on the server clock."""
+    from ipdps26_b200 import engine, gen, serve_trace
+
+    ps = [gen.config5_graph(i) for i in range(args.serve_graphs)]
+    hs = [gen.static(p) for p in ps]
+    t0 = time.perf_counter()
+    trace = serve_trace.make_trace(ps, rate=args.serve_rate, duration=args.serve_seconds, seed=5)
+    out = {
+        "workload": f"config5: {len(hs)} graphs seeds 100-{99 + len(hs)}, |E| log-uniform [1e3, 2e5], "
+                    f"n_nodes=|E|/2, k^-2.5 on [2,25], Zipf-Mandelbrot s=1.2 q={gen.C5_Q:g}; "
+                    f"Poisson {args.serve_rate:g} req/s for {args.serve_seconds:g} s (trace seed 5)",
+        "hyperedges": int(sum(h.n_edges for h in hs)), "requests": len(trace),
+        "update_requests": sum(r.kind == engine.REQ_UPDATE for r in trace),
+        "edits": int(sum(r.edits for r in trace if r.kind == engine.REQ_UPDATE)),
+        "trace_gen_s": time.perf_counter() - t0, "budget_gb": args.serve_budget_gb,
+    }
+    reps = {}
+    for name, mode in (("per_request", engine.SERVE_PER_REQUEST), ("batched", engine.SERVE_BATCHED)):
+        with engine.Server(ctx, mode, mem_budget_bytes=int(args.serve_budget_gb * 1e9)) as srv:
+            for h in hs:
+                srv.add_graph(h.offsets, h.members, h.n_nodes)
+            t0 = time.perf_counter()
+            srv.start()
+            build_s = time.perf_counter() - t0
+            rep = serve_trace.replay(srv, trace)
+            st = srv.stats()
+        reps[name] = rep
+        out[name] = {**serve_trace.summarize(trace, rep), "build_s": build_s, "rounds": int(st.rounds),
+                     "device_gb_after": st.device_bytes / 1e9}
+    out["same_results"] = serve_trace.same_results(reps["per_request"], reps["batched"])
+    out["update_throughput_ratio"] = (out["batched"]["update_batches_per_s"]
+                                      / out["per_request"]["update_batches_per_s"])
+    return out
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -373,9 +420,13 @@ def engine_arm(args, rank, world, local_rank):
         updates = None
         if args.update_batches > 0:
             updates = update_section(args, g, p, counts)
+        g.close()  # the sections below build their own stores
         temporal = None
         if not args.no_temporal:
             temporal = temporal_section(ctx)
+        serve = None
+        if not args.no_serve:
+            serve = serve_section(args, ctx)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
@@ -385,7 +436,7 @@ def engine_arm(args, rank, world, local_rank):
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
                       "device_gb": info.device_bytes / 1e9},
-            "update_batches": updates, "temporal": temporal,
+            "update_batches": updates, "temporal": temporal, "served": serve,
         }
         print(json.dumps(result), flush=True)
     g.close()

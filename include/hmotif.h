@@ -122,6 +122,11 @@ void* hm_ctx_stream(const hm_ctx* ctx);
 /* Test hook: after n further successful device allocations, allocations fail
  * with HM_ERR_NOMEM (n < 0 switches the hook off). */
 int hm_debug_fail_allocations_after(long long n);
+/* Walk order of the touched-triple counts on graph g: 0 = each neighbour's
+ * higher-(degree, id) neighbours (the default, rebuilt after each batch),
+ * 1 = its higher-id neighbours, read straight from the id-sorted rows (what
+ * pooled server stores use). Counts are the same either way; tests run both. */
+int hm_debug_touch_orientation(hm_graph* g, int by_id);
 
 /* ---- the device store ------------------------------------------------- */
 /* Builds H2V (hyperedge -> sorted members), V2H (node -> sorted hyperedges)
@@ -261,6 +266,89 @@ int hm_graph_timings(const hm_graph* g, hm_timings_t* t);
  * of x, y, z; x&y only; y&z only; z&x only; x&y&z. */
 int hm_classify_static(int pattern);
 int hm_classify_temporal(int pattern);
+
+/* ---- Serving: many resident graphs behind one request loop ---------------
+ * No reference counterpart: the reference drivers call applyIncrementalUpdates
+ * + computeMotifCountsDelta (dynamicHyperGraph/src/main.cu:232-244,
+ * src/HMotifCountUpdate.cu:228-301) and computeMotifCounts
+ * (src/HMotifCount.cu:97-125) once per request, which is what
+ * HM_SERVE_PER_REQUEST does here.
+ *
+ * A server owns a set of graphs, each with its own hyperedge ids (0-based,
+ * smallest free id first, exactly as hm_graph_apply_batch assigns them) and
+ * its own node ids. Requests (an update batch with its exact delta, or a full
+ * count) are queued; a loop thread serves them in arrival order per graph.
+ *   HM_SERVE_BATCHED: all graphs live node-disjoint in one pooled store;
+ *     each round the loop admits the oldest waiting request of every graph
+ *     that fits the limits and the memory budget, and serves them all with
+ *     one sequence of launches (the deleted-side count, one store update, one
+ *     touched-triple count that also counts the queried graphs), splitting
+ *     the counters per request. Requests that arrive meanwhile join the next
+ *     round.
+ *   HM_SERVE_PER_REQUEST: one store per graph, one hm_graph_apply_batch /
+ *     hm_count_static30 call per request, in arrival order.
+ * Both give identical results for the same requests. */
+typedef struct hm_server hm_server;
+
+#define HM_SERVE_BATCHED 0
+#define HM_SERVE_PER_REQUEST 1
+
+typedef struct hm_serve_config {
+  int32_t mode;                /* HM_SERVE_BATCHED or HM_SERVE_PER_REQUEST */
+  uint32_t max_batch_requests; /* requests per round, 0 = no limit */
+  uint64_t max_batch_edits;    /* deletions + insertions per round, 0 = no limit */
+  size_t mem_budget_bytes;     /* admission budget, 0 = the context's budget */
+} hm_serve_config;
+
+#define HM_REQ_UPDATE 0
+#define HM_REQ_COUNT 1
+
+typedef struct hm_serve_result {
+  uint64_t ticket;
+  uint32_t graph;
+  int32_t kind;                             /* HM_REQ_UPDATE or HM_REQ_COUNT */
+  int32_t status;                           /* HM_OK or the request's own error */
+  uint32_t n_assigned;                      /* update: ids given to its insertions */
+  int64_t delta30[HM_N_STATIC_CLASSES];     /* update: exact change of the counts */
+  uint64_t counts30[HM_N_STATIC_CLASSES];   /* count: the graph's counts */
+  double submit_ms, start_ms, done_ms;      /* server clock (ms since creation) */
+  uint32_t round_requests;                  /* requests served in its round */
+  uint32_t pad_;
+} hm_serve_result;
+
+typedef struct hm_serve_stats_t {
+  uint64_t rounds;
+  uint64_t requests_done;
+  uint64_t requests_failed;
+  uint64_t edits_done;
+  uint64_t waiting;          /* queued, not yet served */
+  uint64_t deferred_budget;  /* admissions deferred by the memory budget */
+  double busy_ms;            /* loop time spent serving rounds */
+  size_t device_bytes;       /* the context's device memory in use */
+} hm_serve_stats_t;
+
+int hm_serve_create(hm_ctx* ctx, const hm_serve_config* cfg, hm_server** out);
+/* Adds a graph (before hm_serve_start); its id is written to graph_out. */
+int hm_serve_add_graph(hm_server* s, const uint64_t* offsets, const uint32_t* members, uint32_t n_edges,
+                       uint32_t n_nodes, uint32_t* graph_out);
+/* Builds the device stores and starts the loop thread. */
+int hm_serve_start(hm_server* s);
+/* Queue requests; inputs are copied. Validation errors of a request are
+ * reported in its result, and leave its graph unchanged. */
+int hm_serve_submit_update(hm_server* s, uint32_t graph, const uint32_t* del_ids, uint32_t n_del,
+                           const uint64_t* ins_offsets, const uint32_t* ins_members, uint32_t n_ins,
+                           uint64_t* ticket_out);
+int hm_serve_submit_count(hm_server* s, uint32_t graph, uint64_t* ticket_out);
+/* Blocks until the request is served; hands its result over once. assigned
+ * (may be NULL) receives the insertions' ids, up to cap. */
+int hm_serve_wait(hm_server* s, uint64_t ticket, hm_serve_result* out, uint32_t* assigned, uint32_t cap);
+/* Blocks until every queued request has been served. */
+int hm_serve_drain(hm_server* s);
+int hm_serve_stats(hm_server* s, hm_serve_stats_t* out);
+/* Current live ids of one graph (ascending); call when drained. */
+int hm_serve_live_ids(hm_server* s, uint32_t graph, uint32_t* out, uint32_t cap, uint32_t* n_out);
+/* Stops the loop (after serving what is queued) and frees the stores. */
+int hm_serve_destroy(hm_server* s);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,18 @@ i64p = C.POINTER(C.c_int64)
 vp = C.c_void_p
 
 
+# status codes of include/hmotif.h
+HM_OK = 0
+HM_ERR_INVALID = -1
+HM_ERR_CUDA = -2
+HM_ERR_NOMEM = -3
+HM_ERR_CAPACITY = -4
+HM_ERR_NOT_LIVE = -5
+HM_ERR_TIMEOUT = -6
+HM_ERR_STATE = -7
+HM_ERR_LIMIT = -8
+
+
 class HmError(RuntimeError):
     """A negative status returned by the engine."""
 

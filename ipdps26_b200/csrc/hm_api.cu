@@ -84,6 +84,7 @@ extern "C" int hm_graph_destroy(hm_graph* g) {
     CtxLock lock(ctx);
     cudaStreamSynchronize(ctx->stream);
     delete g;
+    hm::trim_pool(ctx);
   }
   return HM_OK;
 }
@@ -193,12 +194,6 @@ extern "C" int hm_classify_temporal(int pattern) {
   return -1;
 }
 
-namespace hm {
-int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
-int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]);
-}  // namespace hm
-
 extern "C" int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32_t n_del,
                                     const uint64_t* ins_offsets, const uint32_t* ins_members, uint32_t n_ins,
                                     uint32_t* assigned_ids_out, int64_t* delta30_out) {
@@ -264,4 +259,10 @@ extern "C" int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N
   if (!g || !out96) return hm::set_error(HM_ERR_INVALID, "hm_count_temporal: NULL argument");
   CtxLock lock(g->ctx);
   return hm::count_temporal96(g, delta, out96);
+}
+
+extern "C" int hm_debug_touch_orientation(hm_graph* g, int by_id) {
+  if (!g) return hm::set_error(HM_ERR_INVALID, "hm_debug_touch_orientation: NULL graph");
+  g->touch_by_id = by_id != 0;
+  return HM_OK;
 }

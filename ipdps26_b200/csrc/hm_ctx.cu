@@ -23,11 +23,21 @@ int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
   if (ctx->budget && now + bytes > ctx->budget)
     return set_error(HM_ERR_NOMEM, "device budget exceeded: %zu used + %zu requested > %zu", now, bytes,
                      ctx->budget);
-  cudaError_t e = cudaMalloc(p, bytes);
+  // Stream-ordered allocation from the context's pool: no device-wide
+  // synchronisation, and freed blocks are reused by the next call. When the
+  // pool cannot grow, its cached free blocks are returned and the request is
+  // retried once.
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
-    return set_error(HM_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    return set_error(HM_ERR_NOMEM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
   }
   ctx->used.fetch_add(bytes);
   return HM_OK;
@@ -35,8 +45,13 @@ int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
 
 void dev_free(hm_ctx* ctx, void* p, size_t bytes) {
   if (!p) return;
-  cudaFree(p);
-  if (ctx) ctx->used.fetch_sub(bytes);
+  cudaFreeAsync(p, ctx->stream);
+  ctx->used.fetch_sub(bytes);
+}
+
+void trim_pool(hm_ctx* ctx) {
+  cudaStreamSynchronize(ctx->stream);
+  cudaMemPoolTrimTo(ctx->pool, 0);
 }
 
 }  // namespace hm
@@ -68,6 +83,19 @@ extern "C" int hm_ctx_create(int device, size_t mem_budget_bytes, hm_ctx** out) 
     delete c;
     return hm::set_error(HM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  e = cudaMemPoolCreate(&c->pool, &props);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return hm::set_error(HM_ERR_CUDA, "cudaMemPoolCreate: %s", cudaGetErrorString(e));
+  }
+  uint64_t keep = UINT64_MAX;  // freed blocks stay cached for the next batch
+  cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   *out = c;
   return HM_OK;
 }
@@ -79,6 +107,7 @@ extern "C" int hm_ctx_destroy(hm_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
   return HM_OK;
 }

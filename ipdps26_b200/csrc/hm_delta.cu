@@ -61,10 +61,15 @@ __global__ void k_list_flagged(const uint32_t* flag, const uint64_t* pos, uint32
     if (flag[i]) out[pos[i]] = (uint32_t)i;
 }
 
+// Counter block of one output row: 30 closed classes, 6 open-pair classes
+// removed by closed triangles, 6 open-pair counts.
+constexpr unsigned kRowStride = 42;
+
 __global__ void __launch_bounds__(kBlock) k_touch_open(const uint32_t* centres, uint32_t n, const uint8_t* mark,
                                                        const uint64_t* off, const uint32_t* len, const uint32_t* nbr,
                                                        const uint8_t* ovl, const uint8_t* esize,
-                                                       unsigned long long* out6) {
+                                                       const uint32_t* gos, const uint32_t* rog,
+                                                       unsigned long long* out) {
   __shared__ uint32_t hist[kWarps][4][256];  // all: type 0/1; unmarked: type 0/1
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint64_t acc[6] = {0, 0, 0, 0, 0, 0};
@@ -101,12 +106,20 @@ __global__ void __launch_bounds__(kBlock) k_touch_open(const uint32_t* centres, 
         for (uint32_t k = 1; k <= s; ++k) hist[w][t][k] += hist[w][t][k - 1];
       open_pair_counts(hist[w][0], hist[w][1], s, acc, false);
       if (!ma) open_pair_counts(hist[w][2], hist[w][3], s, acc, true);
+      if (gos) {  // per-request rows: each centre's pairs go to its graph's row
+        unsigned long long* o = out + (size_t)rog[gos[a]] * kRowStride + 36;
+        for (int k = 0; k < 6; ++k)
+          if (acc[k]) {
+            atomicAdd(&o[k], (unsigned long long)acc[k]);
+            acc[k] = 0;
+          }
+      }
     }
     __syncwarp();
   }
   if (lane == 0)
     for (int k = 0; k < 6; ++k)
-      if (acc[k]) atomicAdd(&out6[k], (unsigned long long)acc[k]);
+      if (acc[k]) atomicAdd(&out[36 + k], (unsigned long long)acc[k]);
 }
 
 __device__ uint32_t triple_overlap3(const uint64_t* hoff, const uint32_t* hmem, const uint8_t* esize, uint32_t a,
@@ -131,7 +144,9 @@ __device__ uint32_t triple_overlap3(const uint64_t* hoff, const uint32_t* hmem, 
 }
 
 struct TouchArgs {
-  const uint32_t* ids;
+  const uint32_t* ids;      // items [0, n_long): slices of rows in global tables
+  uint32_t n_long;
+  const uint32_t* short_ids;  // items [n_long, n): whole rows, heaviest first
   uint32_t n;
   const uint8_t* mark;
   const uint64_t* off;
@@ -151,9 +166,38 @@ struct TouchArgs {
   const uint32_t* gslots;   // per item: slots of that table, 0 for a shared-memory row
   const uint32_t* brange;   // per item: [brange[2i], brange[2i+1]) of row(m) to take b from
   const unsigned long long* gtab;
+  const uint32_t* gos;      // per slot: its graph (null: one output row)
+  const uint32_t* rog;      // per graph: output row
+  bool by_id;               // walk the id-ordered suffix of row(b) instead of N+(b)
   unsigned int* queue;
-  unsigned long long* out;  // 30 closed classes, 6 open-pair removals
+  unsigned long long* out;  // rows of kRowStride counters
 };
+
+// First index of row[0, n) whose value is >= key (or > key with upper),
+// found by the whole warp: 32 probes per round.
+template <bool upper>
+__device__ __forceinline__ uint32_t warp_bound(const uint32_t* row, uint32_t n, uint32_t key) {
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 32) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t p = lo + (lane + 1) * step - 1;
+    bool before = false;
+    if (p < hi) {
+      const uint32_t v = __ldg(row + p);
+      before = upper ? v <= key : v < key;
+    }
+    const uint32_t k = (uint32_t)__popc(__ballot_sync(0xffffffffu, before));
+    lo += k * step;
+    hi = min(hi, lo + step);
+  }
+  bool before = false;
+  if (lo + lane < hi) {
+    const uint32_t v = __ldg(row + lo + lane);
+    before = upper ? v <= key : v < key;
+  }
+  return lo + (uint32_t)__popc(__ballot_sync(0xffffffffu, before));
+}
 
 __device__ __forceinline__ uint32_t size_cat(uint32_t s) { return s >= 3 ? 2u : s - 1u; }
 
@@ -214,12 +258,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= A.n) break;
-    const uint32_t m = A.ids[item];
+    const bool long_row = item < A.n_long;
+    const uint32_t m = long_row ? A.ids[item] : A.short_ids[item - A.n_long];
     const uint64_t mo = A.off[m];
     const uint32_t md = A.len[m];
     const uint32_t sm = A.esize[m];
-    const uint32_t gslots = A.gslots[item];
-    const unsigned long long* gt = A.gtab + A.goff[item];
+    const uint32_t gslots = long_row ? A.gslots[item] : 0u;
+    const unsigned long long* gt = A.gtab + (long_row ? A.goff[item] : 0ull);
     uint32_t shift = 32, bmask = 0;
     if (!gslots) {
       uint32_t slots = 64;
@@ -244,29 +289,35 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     }
     __syncthreads();
     const uint32_t cat_m = size_cat(sm);
-    const uint32_t b_begin = A.brange[2 * item], b_end = A.brange[2 * item + 1];
+    const uint32_t b_begin = long_row ? A.brange[2 * item] : 0u;
+    const uint32_t b_end = long_row ? A.brange[2 * item + 1] : md;
     for (uint32_t bi = b_begin + w; bi < b_end; bi += kWarps) {
       const uint32_t b = A.nbr[mo + bi];
       if (A.mark[b] && b < m) continue;  // counted at b
       const uint32_t cmb = A.ovl[mo + bi];
       const uint32_t sb = A.esize[b];
-      // c runs over N+(b), the neighbours of b ranked above it: each pair
-      // {b, c} of m's neighbours is met once, from its lower-ranked end
-      const uint64_t bo = A.poff[b];
-      const uint32_t bl = A.plen[b];
+      // c runs over the neighbours of b ranked above it: N+(b) by (degree,
+      // id), or the part of b's id-sorted row after b. Each pair {b, c} of
+      // m's neighbours is met once, from its lower-ranked end.
+      uint64_t bo;
+      uint32_t bl;
+      if (A.by_id) {
+        const uint32_t split = warp_bound<true>(A.nbr + A.off[b], A.len[b], b);
+        bo = A.off[b] + split;
+        bl = A.len[b] - split;
+      } else {
+        bo = A.poff[b];
+        bl = A.plen[b];
+      }
+      const uint32_t* cnbr = A.by_id ? A.nbr : A.pnbr;
+      const uint64_t* cmask = A.by_id ? A.mask : A.pmask;
       // masks: relative to m when |m| <= 64, else relative to b when |b| <= 64
       const bool piv_m = sm <= 64, piv_b = !piv_m && sb <= 64;
       uint64_t pmb = piv_m ? A.mask[mo + bi] : 0;
       const uint32_t lo = 0;
       if (piv_b) {  // b's entry for m, from b's full row
         const uint64_t fo = A.off[b];
-        uint32_t l2 = 0, h2 = A.len[b];
-        while (l2 < h2) {
-          const uint32_t mid = (l2 + h2) >> 1;
-          if (A.nbr[fo + mid] < m) l2 = mid + 1;
-          else h2 = mid;
-        }
-        pmb = A.mask[fo + l2];
+        pmb = A.mask[fo + warp_bound<false>(A.nbr + fo, A.len[b], m)];
       }
       const bool star_ok = cmb == 1 && (piv_m || piv_b);
       uint32_t star0 = 0, star1 = 0, star2 = 0;
@@ -278,8 +329,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
           cv[u] = kEmpty;
           ov[u] = 0;
           if (j < bl) {
-            cv[u] = __ldg(A.pnbr + bo + j);
-            ov[u] = __ldg(A.pos + bo + j);
+            cv[u] = __ldg(cnbr + bo + j);
+            ov[u] = A.by_id ? ((uint32_t)__ldg(A.esize + cv[u]) << 8) | __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
           }
         }
 #pragma unroll
@@ -315,7 +366,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
           const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
           uint32_t g;
           if (piv_m || piv_b) {
-            const uint64_t pmc = piv_m ? A.mask[mo + idx] : A.pmask[bo + j0 + u * kWarp + lane];
+            const uint64_t pmc = piv_m ? A.mask[mo + idx] : cmask[bo + j0 + u * kWarp + lane];
             if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
               const uint32_t cc = size_cat(sc);
               star0 += cc == 0;
@@ -358,6 +409,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
       }
       __syncwarp();
     }
+    if (A.gos) {  // per-request rows: flush this item's counts to its graph's row
+      unsigned long long* o = A.out + (size_t)A.rog[A.gos[m]] * kRowStride;
+      for (unsigned k = lane; k < 36; k += kWarp)
+        if (wc[k]) {
+          atomicAdd(&o[k], wc[k]);
+          wc[k] = 0;
+        }
+      __syncwarp();
+    }
     __syncthreads();
   }
   __syncwarp();
@@ -369,16 +429,24 @@ __global__ void k_gather_len(const uint32_t* ids, uint32_t n, const uint32_t* le
   for (uint64_t i = gtid(); i < n; i += gstride()) out[i] = len[ids[i]];
 }
 
+__global__ void k_count_above(const uint32_t* v, uint32_t n, uint32_t limit, unsigned int* out) {
+  for (uint64_t i = gtid(); i < n; i += gstride())
+    if (v[i] > limit) atomicAdd(out, 1u);
+}
+
 constexpr size_t touch_smem() { return (sizeof(uint32_t) + sizeof(uint16_t)) * kSlots; }
 
 }  // namespace
 
-int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]) {
+int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const TouchRows& rows, uint64_t* out) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
-  for (int k = 0; k < 30; ++k) out30[k] = 0;
+  const uint32_t R = rows.gos ? rows.n_rows : 1u;
+  for (size_t k = 0; k < (size_t)R * 30; ++k) out[k] = 0;
   if (!n) return HM_OK;
   const uint32_t E = g->n_slots;
+  const bool by_id = g->touch_by_id;
+  const size_t n_cnt = (size_t)R * kRowStride + 2;  // + queue, + long-row count
   DArr<uint8_t> mark;
   DArr<uint32_t> flag, centres;
   DArr<uint64_t> pos;
@@ -386,18 +454,41 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
   HM_TRY(mark.alloc(ctx, E));
   HM_TRY(flag.alloc(ctx, E));
   HM_TRY(pos.alloc(ctx, (size_t)E + 1));
-  HM_TRY(cnt.alloc(ctx, 44));
+  HM_TRY(cnt.alloc(ctx, n_cnt));
+  unsigned int* queue = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride);
+  unsigned int* n_long_d = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride + 1);
   HM_CUDA(cudaMemsetAsync(mark.p, 0, E, st));
   HM_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(uint32_t) * E, st));
-  HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * 44, st));
+  HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * n_cnt, st));
   k_mark<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, mark.p);
   HM_LAUNCH_CHECK();
   k_flag_touched<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_off.p, g->h2h_len.p,
                                                                        g->h2h_nbr.p, flag.p);
   HM_LAUNCH_CHECK();
   HM_TRY(exclusive_scan(ctx, flag.p, pos.p, E));
+  // marked rows, heaviest first (device sort); rows longer than kRowMax come
+  // first and get global tables
+  DArr<uint32_t> lens, slens, sids;
+  HM_TRY(lens.alloc(ctx, n));
+  HM_TRY(slens.alloc(ctx, n));
+  HM_TRY(sids.alloc(ctx, n));
+  k_gather_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, lens.p);
+  HM_LAUNCH_CHECK();
+  {
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, lens.p, slens.p, d_ids, sids.p, (int64_t)n, 0, 32,
+                                                      st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, lens.p, slens.p, d_ids, sids.p, (int64_t)n, 0, 32,
+                                                      st));
+  }
+  k_count_above<<<grid_for(n, kBlock), kBlock, 0, st>>>(slens.p, n, kRowMax, n_long_d);
+  HM_LAUNCH_CHECK();
   uint64_t nc = 0;
+  unsigned int n_long = 0;
   HM_CUDA(cudaMemcpyAsync(&nc, pos.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaMemcpyAsync(&n_long, n_long_d, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
   HM_TRY(centres.alloc(ctx, nc));
   k_list_flagged<<<grid_for(E, kBlock), kBlock, 0, st>>>(flag.p, pos.p, E, centres.p);
@@ -406,76 +497,65 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
   auto t_open0 = std::chrono::steady_clock::now();
   k_touch_open<<<grid_for(nc * 32, kBlock), kBlock, 0, st>>>(centres.p, (uint32_t)nc, mark.p, g->h2h_off.p,
                                                              g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->esize.p,
-                                                             cnt.p + 36);
+                                                             rows.gos, rows.rog, cnt.p);
   HM_LAUNCH_CHECK();
   static bool attr = false;
   if (!attr) {
     HM_CUDA(cudaFuncSetAttribute(k_touch_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)touch_smem()));
     attr = true;
   }
-  // heaviest rows first; rows longer than kRowMax get a global table
-  DArr<uint32_t> lens;
-  HM_TRY(lens.alloc(ctx, n));
-  k_gather_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, lens.p);
-  HM_LAUNCH_CHECK();
-  std::vector<uint32_t> hid(n), hlen(n), order(n);
-  HM_CUDA(cudaMemcpyAsync(hid.data(), d_ids, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaMemcpyAsync(hlen.data(), lens.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaStreamSynchronize(st));
-  for (uint32_t i = 0; i < n; ++i) order[i] = i;
-  std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return hlen[x] > hlen[y]; });
-  // items: one per marked row held in shared memory; rows in global tables
-  // are split into slices of kSlice neighbours b, one item each
+  // long rows: split into slices of kSlice neighbours b, one item each, all
+  // slices of a row sharing its global table
   constexpr uint32_t kSlice = 256;
   std::vector<uint32_t> oid, oslots, orange;
   std::vector<uint64_t> ooff;
   uint64_t gtotal = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const uint32_t id = hid[order[i]];
-    const uint32_t l = hlen[order[i]];
-    if (l > kRowMax) {
+  if (n_long) {
+    std::vector<uint32_t> hid(n_long), hlen(n_long);
+    HM_CUDA(cudaMemcpyAsync(hid.data(), sids.p, sizeof(uint32_t) * n_long, cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaMemcpyAsync(hlen.data(), slens.p, sizeof(uint32_t) * n_long, cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n_long; ++i) {
       uint32_t sl = 1;
-      while (sl < 2 * l) sl <<= 1;
-      for (uint32_t b0 = 0; b0 < l; b0 += kSlice) {
-        oid.push_back(id);
+      while (sl < 2 * hlen[i]) sl <<= 1;
+      for (uint32_t b0 = 0; b0 < hlen[i]; b0 += kSlice) {
+        oid.push_back(hid[i]);
         oslots.push_back(sl);
         ooff.push_back(gtotal);
         orange.push_back(b0);
-        orange.push_back(std::min(l, b0 + kSlice));
+        orange.push_back(std::min(hlen[i], b0 + kSlice));
       }
       gtotal += sl;
-    } else {
-      oid.push_back(id);
-      oslots.push_back(0);
-      ooff.push_back(0);
-      orange.push_back(0);
-      orange.push_back(l);
     }
   }
-  const uint32_t n_items = (uint32_t)oid.size();
+  const uint32_t n_items_long = (uint32_t)oid.size();
+  const uint32_t n_items = n_items_long + (n - n_long);
   DArr<uint32_t> d_oid, d_oslots, d_orange;
   DArr<uint64_t> d_ooff;
   DArr<unsigned long long> gtab;
-  HM_TRY(d_oid.alloc(ctx, n_items));
-  HM_TRY(d_oslots.alloc(ctx, n_items));
-  HM_TRY(d_orange.alloc(ctx, 2 * (size_t)n_items));
-  HM_TRY(d_ooff.alloc(ctx, n_items));
+  HM_TRY(d_oid.alloc(ctx, n_items_long));
+  HM_TRY(d_oslots.alloc(ctx, n_items_long));
+  HM_TRY(d_orange.alloc(ctx, 2 * (size_t)n_items_long));
+  HM_TRY(d_ooff.alloc(ctx, n_items_long));
   HM_TRY(gtab.alloc(ctx, gtotal ? gtotal : 1));
-  HM_CUDA(cudaMemcpyAsync(d_oid.p, oid.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, st));
-  HM_CUDA(cudaMemcpyAsync(d_oslots.p, oslots.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, st));
-  HM_CUDA(cudaMemcpyAsync(d_orange.p, orange.data(), sizeof(uint32_t) * 2 * n_items, cudaMemcpyHostToDevice, st));
-  HM_CUDA(cudaMemcpyAsync(d_ooff.p, ooff.data(), sizeof(uint64_t) * n_items, cudaMemcpyHostToDevice, st));
-  if (gtotal) {
+  if (n_items_long) {
+    HM_CUDA(cudaMemcpyAsync(d_oid.p, oid.data(), sizeof(uint32_t) * n_items_long, cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaMemcpyAsync(d_oslots.p, oslots.data(), sizeof(uint32_t) * n_items_long, cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaMemcpyAsync(d_orange.p, orange.data(), sizeof(uint32_t) * 2 * n_items_long, cudaMemcpyHostToDevice,
+                            st));
+    HM_CUDA(cudaMemcpyAsync(d_ooff.p, ooff.data(), sizeof(uint64_t) * n_items_long, cudaMemcpyHostToDevice, st));
     HM_CUDA(cudaMemsetAsync(gtab.p, 0xff, sizeof(unsigned long long) * gtotal, st));
-    k_build_ghash<<<grid_for((uint64_t)n_items * 32, kBlock), kBlock, 0, st>>>(
-        d_oid.p, n_items, d_ooff.p, d_oslots.p, d_orange.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, gtab.p);
+    k_build_ghash<<<grid_for((uint64_t)n_items_long * 32, kBlock), kBlock, 0, st>>>(
+        d_oid.p, n_items_long, d_ooff.p, d_oslots.p, d_orange.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, gtab.p);
     HM_LAUNCH_CHECK();
+    // the host copies above read pageable vectors: finish them before they go
+    HM_CUDA(cudaStreamSynchronize(st));
   }
-  if (!g->plus_valid) HM_TRY(build_plus(g));
-  TouchArgs A{d_oid.p, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
-              g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
-              g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
-              reinterpret_cast<unsigned int*>(cnt.p + 42), cnt.p};
+  if (!by_id && !g->plus_valid) HM_TRY(build_plus(g));
+  TouchArgs A{d_oid.p, n_items_long, sids.p + n_long, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+              g->h2h_ovl.p, g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p,
+              g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
+              rows.gos, rows.rog, by_id, queue, cnt.p};
   if (trace) cudaStreamSynchronize(st);
   auto t_cl0 = std::chrono::steady_clock::now();
   k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n_items), kBlock, touch_smem(), st>>>(A);
@@ -483,16 +563,25 @@ int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out3
   if (trace) {
     cudaStreamSynchronize(st);
     const auto t_end = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "[hm_trace touching] marked=%u centres=%llu open=%.1fms closed=%.1fms\n", n,
-                 (unsigned long long)nc, std::chrono::duration<double, std::milli>(t_cl0 - t_open0).count(),
+    std::fprintf(stderr, "[hm_trace touching] marked=%u centres=%llu long=%u by_id=%d open=%.1fms closed=%.1fms\n", n,
+                 (unsigned long long)nc, n_long, (int)by_id,
+                 std::chrono::duration<double, std::milli>(t_cl0 - t_open0).count(),
                  std::chrono::duration<double, std::milli>(t_end - t_cl0).count());
   }
-  unsigned long long h[44];
-  HM_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned long long> h((size_t)R * kRowStride);
+  HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
-  for (int k = 0; k < 30; ++k) out30[k] = h[k];
-  for (int k = 0; k < 6; ++k) out30[20 + k] += h[36 + k] - h[30 + k];
+  for (uint32_t r = 0; r < R; ++r) {
+    const unsigned long long* x = h.data() + (size_t)r * kRowStride;
+    uint64_t* o = out + (size_t)r * 30;
+    for (int k = 0; k < 30; ++k) o[k] = x[k];
+    for (int k = 0; k < 6; ++k) o[20 + k] += x[36 + k] - x[30 + k];
+  }
   return HM_OK;
+}
+
+int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]) {
+  return count_touching_rows(g, d_ids, n, TouchRows{}, out30);
 }
 
 }  // namespace hm

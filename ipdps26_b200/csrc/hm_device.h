@@ -33,6 +33,7 @@ struct hm_ctx {
   size_t budget = 0;  // bytes; 0 = all free memory at creation
   std::atomic<size_t> used{0};
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;  // every device array of the context, stream-ordered on `stream`
   int n_sms = 148;
   std::mutex mu;  // serialises calls that share this context
 };
@@ -41,6 +42,7 @@ namespace hm {
 
 int dev_alloc(hm_ctx* ctx, void** p, size_t bytes);
 void dev_free(hm_ctx* ctx, void* p, size_t bytes);
+void trim_pool(hm_ctx* ctx);  // returns the pool's cached free blocks to the device
 
 // Owning device array; the context's budget is charged for its bytes.
 template <class T>
@@ -129,6 +131,9 @@ struct hm_graph {
 
   // oriented adjacency (rebuilt lazily after updates)
   bool plus_valid = false;
+  // touched-triple counts walk id-ordered row suffixes instead of N+ (no
+  // oriented copy to rebuild after each batch; used by pooled stores)
+  bool touch_by_id = false;
   hm::DArr<uint64_t> plus_off;
   hm::DArr<uint32_t> plus_len;
   hm::DArr<uint32_t> plus_nbr;
@@ -177,6 +182,16 @@ int build_h2h_rows(hm_graph* g);
 int h2h_rows_for(hm_graph* g, const uint32_t* d_rows, uint32_t n_rows,
                  const std::function<int(uint64_t, uint64_t*)>& reserve, uint64_t* written);
 int build_plus(hm_graph* g);
+// Oriented rows of a subset of slots (indexed by slot; only listed slots valid).
+struct PlusRows {
+  DArr<uint64_t> off;
+  DArr<uint32_t> len;
+  DArr<uint32_t> nbr;
+  DArr<uint16_t> os;
+  DArr<uint64_t> mask;
+  uint64_t nnz = 0;
+};
+int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P);
 template <class T>
 int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n);
 
@@ -185,6 +200,30 @@ int prepare_static(hm_graph* g);
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags);
 int finish_static(hm_graph* g, uint64_t out30[30]);
 int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
+
+// Touched-triple counts (hm_delta.cu). With gos set, the triples of each
+// touched hyperedge's graph gos[slot] go to output row rog[gos[slot]]
+// (n_rows rows of 30); the graphs of one call must not share hyperedges'
+// neighbourhoods (pooled graphs are node-disjoint).
+struct TouchRows {
+  const uint32_t* gos = nullptr;
+  const uint32_t* rog = nullptr;
+  uint32_t n_rows = 1;
+};
+int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const TouchRows& rows, uint64_t* out);
+int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]);
+// Full counts of the graphs whose every live slot is listed (hm_static.cu).
+int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const TouchRows& rows, uint64_t* out);
+
+// Batch updates (hm_update.cu).
+struct BatchHooks {
+  std::function<int(const uint32_t* d_dels, uint32_t n_del)> before;  // old graph, deleted slots
+  std::function<int(const uint32_t* d_ins, uint32_t n_ins)> after;    // new graph, assigned slots
+};
+int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
+                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks);
+int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
+                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
 
 inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
   uint64_t b = (items + per_block - 1) / per_block;

@@ -58,17 +58,28 @@ __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
 
 // ---- phase 1: all neighbour pairs of each centre, classified as open --------
 
+// Counter block of one output row: 30 closed classes, 6 open-pair classes
+// removed by closed triangles, 6 open-pair counts (per-request rows of a
+// pooled store use one block each).
+constexpr unsigned kRowStride = 42;
+
+// centres == nullptr: every slot 0..n-1 is a centre; else the n listed ones.
+// With gos set, each centre's pairs go to row rog[gos[a]] of out6's blocks.
 __global__ void __launch_bounds__(kOpenBlock) k_open_pairs(const uint64_t* __restrict__ off,
                                                            const uint32_t* __restrict__ len,
                                                            const uint32_t* __restrict__ nbr,
                                                            const uint8_t* __restrict__ ovl,
-                                                           const uint8_t* __restrict__ esize, uint32_t n,
+                                                           const uint8_t* __restrict__ esize,
+                                                           const uint32_t* __restrict__ centres, uint32_t n,
                                                            uint32_t shard, uint32_t n_shards,
+                                                           const uint32_t* __restrict__ gos,
+                                                           const uint32_t* __restrict__ rog,
                                                            unsigned long long* __restrict__ out6) {
   __shared__ uint32_t hist[kOpenWarps][2][256];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint64_t acc[6] = {0, 0, 0, 0, 0, 0};  // lane 0's running class counts
-  for (uint64_t a = shard + global_warp() * n_shards; a < n; a += n_warps() * n_shards) {
+  for (uint64_t i = shard + global_warp() * n_shards; i < n; i += n_warps() * n_shards) {
+    const uint32_t a = centres ? centres[i] : (uint32_t)i;
     const uint32_t l = len[a];
     if (l < 2) continue;
     const uint32_t s = esize[a];
@@ -102,6 +113,14 @@ __global__ void __launch_bounds__(kOpenBlock) k_open_pairs(const uint64_t* __res
         h1[k] += h1[k - 1];
       }
       open_pair_counts(h0, h1, s, acc, false);
+      if (gos) {
+        unsigned long long* o = out6 + (size_t)rog[gos[a]] * kRowStride;
+        for (int k = 0; k < 6; ++k)
+          if (acc[k]) {
+            atomicAdd(&o[k], (unsigned long long)acc[k]);
+            acc[k] = 0;
+          }
+      }
     }
     __syncwarp();
   }
@@ -125,8 +144,10 @@ struct ClosedArgs {
   uint32_t n_work;
   uint32_t shard, n_shards;  // this call takes work items shard, shard + n_shards, ...
   unsigned int* queue;
-  unsigned long long* out;  // kNumCounters
+  unsigned long long* out;  // kNumCounters (rows of kRowStride with gos)
   uint8_t* edge_flags;      // diagnostics only: marks oriented entries that close a triangle
+  const uint32_t* gos;      // per slot: its graph (null: one output row)
+  const uint32_t* rog;      // per graph: output row
 };
 
 // |a & b & c| by a three-way merge of the member lists (centres with more
@@ -348,6 +369,15 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       }
       __syncwarp();
     }
+    if (A.gos) {  // per-request rows: this centre's triangles go to its graph's row
+      unsigned long long* o = A.out + (size_t)A.rog[A.gos[a]] * kRowStride;
+      for (unsigned k = lane; k < kNumCounters; k += kWarp)
+        if (wc[k]) {
+          atomicAdd(&o[k], wc[k]);
+          wc[k] = 0;
+        }
+      __syncwarp();
+    }
     __syncthreads();
   }
   __syncwarp();
@@ -359,9 +389,10 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
 // than two oriented neighbours own no triangle and are dropped (key 0). Rows
 // longer than kSmallRow get the top bit so they sort first and go to the
 // large-table launch.
-__global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, uint32_t n,
-                              uint64_t* est, uint32_t* ids) {
-  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+__global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, const uint32_t* rows,
+                              uint32_t n, uint64_t* est, uint32_t* ids) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint32_t d = plen[a];
     uint64_t s = 0;
     if (d >= 2)
@@ -370,8 +401,8 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
     if (lane_id() == 0) {
       uint64_t key = (d >= 2 && s > 0) ? s + d : 0;
       if (key && d > kSmallRow) key |= 1ull << 63;
-      est[a] = key;
-      ids[a] = (uint32_t)a;
+      est[r] = key;
+      ids[r] = a;
     }
   }
 }
@@ -392,8 +423,8 @@ static int closed_worklist(hm_graph* g) {
   HM_TRY(est_sorted.alloc(ctx, E));
   HM_TRY(ids.alloc(ctx, E));
   HM_TRY(g->work.alloc(ctx, E));
-  k_closed_work<<<grid_for((uint64_t)E * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p, E,
-                                                                est.p, ids.p);
+  k_closed_work<<<grid_for((uint64_t)E * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p,
+                                                                nullptr, E, est.p, ids.p);
   HM_LAUNCH_CHECK();
   size_t tb = 0;
   HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, g->work.p, (int64_t)E,
@@ -425,6 +456,18 @@ static int closed_worklist(hm_graph* g) {
   return HM_OK;
 }
 
+static int prepare_static_attrs() {
+  static bool attr_set = false;
+  if (!attr_set) {
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kBigSlots)));
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kSmallSlots)));
+    attr_set = true;
+  }
+  return HM_OK;
+}
+
 // Everything the count kernels need that only changes with the graph.
 int prepare_static(hm_graph* g) {
   hm_ctx* ctx = g->ctx;
@@ -438,15 +481,7 @@ int prepare_static(hm_graph* g) {
     for (auto& e : g->ev) HM_CUDA(cudaEventCreate(&e));
     g->ev_ready = true;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)closed_smem_bytes(kBigSlots)));
-    HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)closed_smem_bytes(kSmallSlots)));
-    attr_set = true;
-  }
-  return HM_OK;
+  return prepare_static_attrs();
 }
 
 // Launches both phases for one shard of the centres; the counters land in
@@ -461,8 +496,8 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   HM_CUDA(cudaEventRecord(g->ev[0], st));
   if (E) {
     k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
-                                                                 g->h2h_ovl.p, g->esize.p, E, shard, n_shards,
-                                                                 dev + 36);
+                                                                 g->h2h_ovl.p, g->esize.p, nullptr, E, shard,
+                                                                 n_shards, nullptr, nullptr, dev + 36);
     HM_LAUNCH_CHECK();
   }
   HM_CUDA(cudaEventRecord(g->ev[1], st));
@@ -474,7 +509,7 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
     if (n <= shard) continue;
     ClosedArgs A{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p,
                  g->esize.p, g->work.p + begin, n, shard, n_shards,
-                 reinterpret_cast<unsigned int*>(dev + 42 + part), dev, edge_flags};
+                 reinterpret_cast<unsigned int*>(dev + 42 + part), dev, edge_flags, nullptr, nullptr};
     const uint32_t items = (n - shard + n_shards - 1) / n_shards;
     if (part == 0) {
       const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
@@ -507,6 +542,89 @@ int finish_static(hm_graph* g, uint64_t out30[30]) {
   }
   for (int k = 0; k < 6; ++k) out30[20 + k] += h[36 + k] - h[30 + k];
   g->times.closed_triangles = tri;
+  return HM_OK;
+}
+
+namespace {
+__global__ void k_count_work(const uint64_t* est, uint32_t n, unsigned int* out2) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (est[i]) atomicAdd(&out2[0], 1u);
+    if (est[i] >> 63) atomicAdd(&out2[1], 1u);
+  }
+}
+}  // namespace
+
+// Full counts of the graphs behind the listed slots (every live slot of each
+// counted graph, graphs node-disjoint): the static algorithm over the listed
+// centres only, with oriented rows built for them alone and each centre's
+// counts routed to row rog[gos[a]] of out (n_rows x 30).
+int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const TouchRows& rows, uint64_t* out) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t R = rows.n_rows;
+  for (size_t k = 0; k < (size_t)R * 30; ++k) out[k] = 0;
+  if (!n) return HM_OK;
+  HM_TRY(prepare_static_attrs());
+  PlusRows P;
+  HM_TRY(build_plus_rows(g, d_rows, n, &P));
+  DArr<uint64_t> est, est_sorted;
+  DArr<uint32_t> ids, work;
+  DArr<unsigned long long> cnt;
+  const size_t n_cnt = (size_t)R * kRowStride + 4;  // + two queues, + two work counts
+  HM_TRY(est.alloc(ctx, n));
+  HM_TRY(est_sorted.alloc(ctx, n));
+  HM_TRY(ids.alloc(ctx, n));
+  HM_TRY(work.alloc(ctx, n));
+  HM_TRY(cnt.alloc(ctx, n_cnt));
+  HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * n_cnt, st));
+  unsigned long long* tail = cnt.p + (size_t)R * kRowStride;
+  k_closed_work<<<grid_for((uint64_t)n * 32, 256), 256, 0, st>>>(P.off.p, P.len.p, P.nbr.p, d_rows, n, est.p, ids.p);
+  HM_LAUNCH_CHECK();
+  {
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, work.p, (int64_t)n, 0,
+                                                      64, st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, est.p, est_sorted.p, ids.p, work.p, (int64_t)n, 0,
+                                                      64, st));
+  }
+  unsigned int* wc = reinterpret_cast<unsigned int*>(tail + 2);
+  k_count_work<<<grid_for(n, 256), 256, 0, st>>>(est_sorted.p, n, wc);
+  HM_LAUNCH_CHECK();
+  k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                               g->h2h_ovl.p, g->esize.p, d_rows, n, 0, 1, rows.gos,
+                                                               rows.rog, cnt.p + 36);
+  HM_LAUNCH_CHECK();
+  unsigned int hw[2] = {0, 0};
+  HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  const uint32_t n_work = hw[0], n_big = hw[1];
+  for (int part = 0; part < 2; ++part) {
+    const uint32_t begin = part ? n_big : 0, end = part ? n_work : n_big;
+    const uint32_t m = end - begin;
+    if (!m) continue;
+    ClosedArgs A{P.off.p, P.len.p, P.nbr.p, P.os.p, P.mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p,
+                 work.p + begin, m, 0, 1, reinterpret_cast<unsigned int*>(tail + part), cnt.p, nullptr, rows.gos,
+                 rows.rog};
+    if (part == 0) {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, m);
+      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
+    } else {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, m);
+      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
+    }
+    HM_LAUNCH_CHECK();
+  }
+  std::vector<unsigned long long> h((size_t)R * kRowStride);
+  HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t r = 0; r < R; ++r) {
+    const unsigned long long* x = h.data() + (size_t)r * kRowStride;
+    uint64_t* o = out + (size_t)r * 30;
+    for (int k = 0; k < 30; ++k) o[k] = x[k];
+    for (int k = 0; k < 6; ++k) o[20 + k] += x[36 + k] - x[30 + k];
+  }
   return HM_OK;
 }
 

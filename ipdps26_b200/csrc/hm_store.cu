@@ -242,9 +242,12 @@ __device__ __forceinline__ bool above(uint32_t a, uint32_t da, uint32_t b, uint3
   return db > da || (db == da && b > a);
 }
 
-__global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, uint32_t n,
-                             uint32_t* cnt) {
-  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+// rows == nullptr: rows 0..n-1; else the listed rows. cnt[i] is the i-th
+// row's count.
+__global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint32_t* rows,
+                             uint32_t n, uint32_t* cnt) {
+  for (uint64_t i = global_warp(); i < n; i += n_warps()) {
+    const uint32_t a = rows ? rows[i] : (uint32_t)i;
     const uint64_t s = off[a];
     const uint32_t l = len[a];
     uint32_t c = 0;
@@ -253,18 +256,19 @@ __global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uin
       bool up = false;
       if (i < l) {
         const uint32_t b = nbr[s + i];
-        up = above((uint32_t)a, l, b, len[b]);
+        up = above(a, l, b, len[b]);
       }
       c += __popc(__ballot_sync(0xffffffffu, up));
     }
-    if (lane_id() == 0) cnt[a] = c;
+    if (lane_id() == 0) cnt[i] = c;
   }
 }
 
 __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint8_t* ovl,
-                             const uint64_t* mask, const uint8_t* esize, uint32_t n, const uint64_t* poff,
-                             uint32_t* pnbr, uint16_t* pos, uint64_t* pmask) {
-  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+                             const uint64_t* mask, const uint8_t* esize, const uint32_t* rows, uint32_t n,
+                             const uint64_t* poff, uint32_t* pnbr, uint16_t* pos, uint64_t* pmask) {
+  for (uint64_t r = global_warp(); r < n; r += n_warps()) {
+    const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint64_t s = off[a];
     const uint32_t l = len[a];
     uint64_t w = poff[a];
@@ -274,7 +278,7 @@ __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uin
       uint32_t b = 0;
       if (i < l) {
         b = nbr[s + i];
-        up = above((uint32_t)a, l, b, len[b]);
+        up = above(a, l, b, len[b]);
       }
       const unsigned m = __ballot_sync(0xffffffffu, up);
       if (up) {
@@ -564,6 +568,50 @@ int build_h2h_rows(hm_graph* g) {
   return HM_OK;
 }
 
+__global__ void k_plus_scatter(const uint32_t* rows, uint32_t n, const uint64_t* pos, const uint32_t* cnt,
+                               uint64_t* poff, uint32_t* plen) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    poff[rows[i]] = pos[i];
+    plen[rows[i]] = cnt[i];
+  }
+}
+
+// Oriented rows of the listed slots only, in a set of their own (entries of
+// other slots are not written). Enough for counts whose triangles stay among
+// the listed slots, as a pooled graph's do.
+int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  DArr<uint32_t> cnt;
+  DArr<uint64_t> pos;
+  HM_TRY(cnt.alloc(ctx, n));
+  HM_TRY(pos.alloc(ctx, (size_t)n + 1));
+  HM_TRY(P->off.alloc(ctx, (size_t)g->n_slots + 1));
+  HM_TRY(P->len.alloc(ctx, g->n_slots));
+  if (n) {
+    k_plus_count<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                      d_rows, n, cnt.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(exclusive_scan(ctx, cnt.p, pos.p, n));
+  uint64_t total = 0;
+  HM_CUDA(cudaMemcpyAsync(&total, pos.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  HM_TRY(P->nbr.alloc(ctx, total));
+  HM_TRY(P->os.alloc(ctx, total));
+  HM_TRY(P->mask.alloc(ctx, total));
+  if (n) {
+    k_plus_scatter<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_rows, n, pos.p, cnt.p, P->off.p, P->len.p);
+    HM_LAUNCH_CHECK();
+    k_plus_write<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                      g->h2h_ovl.p, g->h2h_mask.p, g->esize.p, d_rows,
+                                                                      n, P->off.p, P->nbr.p, P->os.p, P->mask.p);
+    HM_LAUNCH_CHECK();
+  }
+  P->nnz = total;
+  return HM_OK;
+}
+
 int build_plus(hm_graph* g) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
@@ -571,8 +619,8 @@ int build_plus(hm_graph* g) {
   DArr<uint32_t> cnt;
   HM_TRY(cnt.alloc(ctx, E));
   if (E) {
-    k_plus_count<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, E,
-                                                                      cnt.p);
+    k_plus_count<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                      nullptr, E, cnt.p);
     HM_LAUNCH_CHECK();
   }
   HM_TRY(g->plus_off.alloc(ctx, (size_t)E + 1));
@@ -585,9 +633,9 @@ int build_plus(hm_graph* g) {
   HM_TRY(g->plus_mask.alloc(ctx, total));
   if (E) {
     k_plus_write<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
-                                                                      g->h2h_ovl.p, g->h2h_mask.p, g->esize.p, E,
-                                                                      g->plus_off.p, g->plus_nbr.p, g->plus_os.p,
-                                                                      g->plus_mask.p);
+                                                                      g->h2h_ovl.p, g->h2h_mask.p, g->esize.p,
+                                                                      nullptr, E, g->plus_off.p, g->plus_nbr.p,
+                                                                      g->plus_os.p, g->plus_mask.p);
     HM_LAUNCH_CHECK();
   }
   g->plus_len = static_cast<DArr<uint32_t>&&>(cnt);

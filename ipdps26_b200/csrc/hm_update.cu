@@ -576,8 +576,6 @@ static int compact_h2v(hm_graph* g, uint64_t extra) {
   return HM_OK;
 }
 
-int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]);
-
 // Per-phase wall times of one batch, printed to stderr when HM_TRACE is set
 // in the environment (each mark synchronises the stream; diagnostics only).
 struct PhaseTrace {
@@ -605,10 +603,11 @@ struct PhaseTrace {
   }
 };
 
-// Deletes, inserts, and optionally reports the exact change of the 30 static
-// classes. All device work; the host only sequences the kernels.
-int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30) {
+// Deletes and inserts; hooks.before sees the old graph and the deleted slots,
+// hooks.after the new graph and the assigned slots (both device arrays). All
+// device work; the host only sequences the kernels.
+int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
+                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   if (g->temporal) return set_error(HM_ERR_STATE, "apply_batch: temporal graphs are immutable");
@@ -651,12 +650,7 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
 
   PhaseTrace trace(st);
   trace.mark("validate");
-  int64_t before[30] = {0};
-  if (delta30 && n_del) {
-    uint64_t c[30];
-    HM_TRY(count_touching(g, dels.p, n_del, c));
-    for (int k = 0; k < 30; ++k) before[k] = (int64_t)c[k];
-  }
+  if (hooks.before) HM_TRY(hooks.before(dels.p, n_del));
   trace.mark("count_deleted");
 
   // ---- deletions: H2H removal patches from the rows about to vanish ----------
@@ -933,11 +927,9 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
   g->work_valid = false;
 
   trace.mark("bookkeeping");
-  if (delta30) {
-    uint64_t c[30] = {0};
-    if (n_ins) HM_TRY(count_touching(g, ids.p, n_ins, c));
+  if (hooks.after) {
+    HM_TRY(hooks.after(ids.p, n_ins));
     trace.mark("count_inserted");
-    for (int k = 0; k < 30; ++k) delta30[k] = (int64_t)c[k] - before[k];
   }
   HM_CUDA(cudaEventRecord(e1, st));
   HM_CUDA(cudaEventSynchronize(e1));
@@ -946,6 +938,20 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
   g->times.update_ms = ms;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return HM_OK;
+}
+
+// Exact change of the 30 static classes: touched triples of the inserted
+// hyperedges in the new graph minus those of the deleted ones in the old.
+int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
+                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30) {
+  if (!delta30) return apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, BatchHooks{});
+  uint64_t before[30] = {0}, after[30] = {0};
+  BatchHooks hooks;
+  hooks.before = [&](const uint32_t* d, uint32_t n) { return n ? count_touching(g, d, n, before) : (int)HM_OK; };
+  hooks.after = [&](const uint32_t* d, uint32_t n) { return n ? count_touching(g, d, n, after) : (int)HM_OK; };
+  HM_TRY(apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, hooks));
+  for (int k = 0; k < 30; ++k) delta30[k] = (int64_t)(after[k] - before[k]);
   return HM_OK;
 }
 

@@ -57,6 +57,45 @@ class Timings(C.Structure):
     ]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("max_batch_requests", C.c_uint32),
+        ("max_batch_edits", C.c_uint64),
+        ("mem_budget_bytes", C.c_size_t),
+    ]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("graph", C.c_uint32),
+        ("kind", C.c_int32),
+        ("status", C.c_int32),
+        ("n_assigned", C.c_uint32),
+        ("delta30", C.c_int64 * 30),
+        ("counts30", C.c_uint64 * 30),
+        ("submit_ms", C.c_double),
+        ("start_ms", C.c_double),
+        ("done_ms", C.c_double),
+        ("round_requests", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("rounds", C.c_uint64),
+        ("requests_done", C.c_uint64),
+        ("requests_failed", C.c_uint64),
+        ("edits_done", C.c_uint64),
+        ("waiting", C.c_uint64),
+        ("deferred_budget", C.c_uint64),
+        ("busy_ms", C.c_double),
+        ("device_bytes", C.c_size_t),
+    ]
+
+
 _lib.bind(
     {
         "hm_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(vp)]),
@@ -77,6 +116,18 @@ _lib.bind(
         "hm_graph_live_ids": (C.c_int, [vp, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_count_touching30": (C.c_int, [vp, u32p, C.c_uint32, u64p]),
         "hm_count_temporal": (C.c_int, [vp, C.c_int64, u64p]),
+        "hm_debug_touch_orientation": (C.c_int, [vp, C.c_int]),
+        "hm_serve_create": (C.c_int, [vp, C.POINTER(ServeConfig), C.POINTER(vp)]),
+        "hm_serve_add_graph": (C.c_int, [vp, u64p, u32p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "hm_serve_start": (C.c_int, [vp]),
+        "hm_serve_submit_update": (C.c_int, [vp, C.c_uint32, u32p, C.c_uint32, u64p, u32p, C.c_uint32,
+                                             C.POINTER(C.c_uint64)]),
+        "hm_serve_submit_count": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_uint64)]),
+        "hm_serve_wait": (C.c_int, [vp, C.c_uint64, C.POINTER(ServeResult), u32p, C.c_uint32]),
+        "hm_serve_drain": (C.c_int, [vp]),
+        "hm_serve_stats": (C.c_int, [vp, C.POINTER(ServeStats)]),
+        "hm_serve_live_ids": (C.c_int, [vp, C.c_uint32, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "hm_serve_destroy": (C.c_int, [vp]),
         "hm_classify_static": (C.c_int, [C.c_int]),
         "hm_classify_temporal": (C.c_int, [C.c_int]),
     }
@@ -216,6 +267,10 @@ class Graph:
               "hm_count_touching30")
         return out
 
+    def set_touch_orientation(self, by_id: bool) -> None:
+        """Walk order of the touched-triple counts (same counts either way)."""
+        check(lib.hm_debug_touch_orientation(self._h, int(by_id)), "hm_debug_touch_orientation")
+
     def query(self, ids) -> list[np.ndarray]:
         ids = np.ascontiguousarray(ids, dtype=np.uint32)
         n = len(ids)
@@ -229,6 +284,98 @@ class Graph:
     def close(self) -> None:
         if self._h:
             lib.hm_graph_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+SERVE_BATCHED = 0
+SERVE_PER_REQUEST = 1
+REQ_UPDATE = 0
+REQ_COUNT = 1
+
+
+class Server:
+    """Many resident graphs behind one request loop (hm_serve_* in hmotif.h).
+
+    ``mode`` SERVE_BATCHED serves one request of every waiting graph per
+    round over a pooled store; SERVE_PER_REQUEST serves them one call at a
+    time on per-graph stores. Results are the same.
+    """
+
+    def __init__(self, ctx: Context, mode: int = SERVE_BATCHED, max_batch_requests: int = 0,
+                 max_batch_edits: int = 0, mem_budget_bytes: int = 0):
+        cfg = ServeConfig(mode, max_batch_requests, max_batch_edits, mem_budget_bytes)
+        h = vp()
+        check(lib.hm_serve_create(ctx.handle, C.byref(cfg), C.byref(h)), "hm_serve_create")
+        self._h = h
+        self.ctx = ctx
+        self.mode = mode
+        ctx._children.add(self)
+
+    def add_graph(self, offsets, members, n_nodes: int) -> int:
+        off, mem = _csr_arrays(offsets, members)
+        gid = C.c_uint32()
+        check(lib.hm_serve_add_graph(self._h, ptr(off, C.c_uint64),
+                                     ptr(mem if len(mem) else np.zeros(1, np.uint32), C.c_uint32), len(off) - 1,
+                                     int(n_nodes), C.byref(gid)), "hm_serve_add_graph")
+        return gid.value
+
+    def start(self) -> None:
+        check(lib.hm_serve_start(self._h), "hm_serve_start")
+
+    def submit_update(self, graph: int, del_ids=None, ins_offsets=None, ins_members=None) -> int:
+        d = np.ascontiguousarray(del_ids if del_ids is not None else [], dtype=np.uint32)
+        if ins_offsets is None:
+            ins_offsets, ins_members = np.zeros(1, np.uint64), np.zeros(0, np.uint32)
+        off, mem = _csr_arrays(ins_offsets, ins_members)
+        t = C.c_uint64()
+        check(lib.hm_serve_submit_update(self._h, graph, ptr(d if len(d) else np.zeros(1, np.uint32), C.c_uint32),
+                                         len(d), ptr(off, C.c_uint64),
+                                         ptr(mem if len(mem) else np.zeros(1, np.uint32), C.c_uint32), len(off) - 1,
+                                         C.byref(t)), "hm_serve_submit_update")
+        return t.value
+
+    def submit_count(self, graph: int) -> int:
+        t = C.c_uint64()
+        check(lib.hm_serve_submit_count(self._h, graph, C.byref(t)), "hm_serve_submit_count")
+        return t.value
+
+    def wait(self, ticket: int, cap: int = 1 << 20):
+        """(ServeResult, assigned ids) of a request; blocks until served."""
+        r = ServeResult()
+        ids = np.zeros(max(cap, 1), np.uint32)
+        check(lib.hm_serve_wait(self._h, ticket, C.byref(r), ptr(ids, C.c_uint32), cap), "hm_serve_wait")
+        return r, ids[: r.n_assigned].copy()
+
+    def drain(self) -> None:
+        check(lib.hm_serve_drain(self._h), "hm_serve_drain")
+
+    def stats(self) -> ServeStats:
+        s = ServeStats()
+        check(lib.hm_serve_stats(self._h, C.byref(s)), "hm_serve_stats")
+        return s
+
+    def live_ids(self, graph: int) -> np.ndarray:
+        n = C.c_uint32()
+        cap = 1 << 22
+        out = np.zeros(cap, np.uint32)
+        check(lib.hm_serve_live_ids(self._h, graph, ptr(out, C.c_uint32), cap, C.byref(n)), "hm_serve_live_ids")
+        return out[: n.value].copy()
+
+    def close(self) -> None:
+        if self._h:
+            lib.hm_serve_destroy(self._h)
             self._h = None
 
     def __enter__(self):

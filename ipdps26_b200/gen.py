@@ -92,7 +92,8 @@ def config1(seed: int = 0, n_nodes: int = 10_000, n_edges: int = 20_000, q: floa
 
 # Config 2: 1M nodes, 2M hyperedges, sizes k^-2.2 on [2,100], Zipf-Mandelbrot
 # s = 1.1 with offset q = 1000 (plain Zipf(1.1) makes the projection of this
-# size exceed device memory and any exact counter).
+# size exceed device memory and any exact counter: a hub of degree ~770K and
+# about 1.1e17 triples sharing one node).
 C2_Q = 1000.0
 
 
@@ -104,3 +105,19 @@ def config2(seed: int = 1, n_nodes: int = 1_000_000, n_edges: int = 2_000_000, q
 # [2,20], Zipf(1.2); repeated node-sets are kept (they make motifs 87-96).
 def config4(seed: int = 3, n_nodes: int = 200_000, n_edges: int = 500_000, q: float = 0.0) -> GenParams:
     return params(seed, n_nodes, n_edges, 2, 20, 2.5, 1.2, q, dedupe=False)
+
+
+# Config 5: resident graphs with |E| log-uniform in [1e3, 2e5] (seeds 100 +
+# i), n_nodes = |E| / 2, config-1 size law (k^-2.5 on [2, 25]) and Zipf(1.2)
+# popularity with the Zipf-Mandelbrot offset q = 1000 of config 2 (with q = 0
+# a 200K-edge graph has a hub in about half of its hyperedges and ~1.8e14
+# triples sharing one node, hours of exact counting per request).
+C5_Q = 1000.0
+
+
+def config5_graph(i: int, e_min: int = 1000, e_max: int = 200_000, q: float = C5_Q) -> GenParams:
+    seed = 100 + i
+    u = np.random.default_rng(seed).uniform(np.log(e_min), np.log(e_max))
+    n_edges = int(round(np.exp(u)))
+    return params(seed, max(n_edges // 2, 2), n_edges, 2, 25, 2.5, 1.2, q)
+

@@ -82,3 +82,49 @@ def test_cpp_shim_compiles_and_links(tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert subprocess.run([str(out)]).returncode == 0
+
+
+def test_struct_layouts_match_ctypes(tmp_path):
+    """The ctypes mirrors in engine.py have the C structs' sizes and field
+    offsets (checked by compiling a probe against include/hmotif.h)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    from ipdps26_b200 import engine
+
+    cc = shutil.which("gcc")
+    if cc is None:
+        return
+    structs = {
+        "hm_graph_info_t": engine.GraphInfo, "hm_traffic_t": engine.Traffic, "hm_timings_t": engine.Timings,
+        "hm_serve_config": engine.ServeConfig, "hm_serve_result": engine.ServeResult,
+        "hm_serve_stats_t": engine.ServeStats,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hmotif.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run([cc, f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, f, v = ln.split()
+        got[(cname, f)] = int(v)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_status_constants_match_header():
+    from ipdps26_b200 import _lib
+
+    text = (ROOT / "include" / "hmotif.h").read_text()
+    for m in re.finditer(r"#define (HM_(?:OK|ERR_\w+))\s+\(?(-?\d+)\)?", text):
+        assert getattr(_lib, m.group(1)) == int(m.group(2)), m.group(1)
