@@ -425,13 +425,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     if (wc[k]) atomicAdd(&A.out[k], wc[k]);
 }
 
-__global__ void k_gather_len(const uint32_t* ids, uint32_t n, const uint32_t* len, uint32_t* out) {
-  for (uint64_t i = gtid(); i < n; i += gstride()) out[i] = len[ids[i]];
+// Sort key of a marked row: [long row] [output row of its graph when gos is
+// set, 31 bits] [row length, 32 bits]. Descending order puts rows in global
+// tables first, then keeps each graph's rows together (heaviest first), so
+// that the blocks running at one time share one graph's rows in L2.
+__global__ void k_touch_keys(const uint32_t* ids, uint32_t n, const uint32_t* len, const uint32_t* gos,
+                             const uint32_t* rog, uint64_t* key) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const uint32_t m = ids[i], l = len[m];
+    uint64_t k = l;
+    if (gos) k |= (uint64_t)min(rog[gos[m]], 0x7fffffffu) << 32;
+    if (l > kRowMax) k |= 1ull << 63;
+    key[i] = k;
+  }
 }
 
-__global__ void k_count_above(const uint32_t* v, uint32_t n, uint32_t limit, unsigned int* out) {
+__global__ void k_count_long(const uint64_t* key, uint32_t n, unsigned int* out) {
   for (uint64_t i = gtid(); i < n; i += gstride())
-    if (v[i] > limit) atomicAdd(out, 1u);
+    if (key[i] >> 63) atomicAdd(out, 1u);
 }
 
 constexpr size_t touch_smem() { return (sizeof(uint32_t) + sizeof(uint16_t)) * kSlots; }
@@ -468,22 +479,23 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   HM_TRY(exclusive_scan(ctx, flag.p, pos.p, E));
   // marked rows, heaviest first (device sort); rows longer than kRowMax come
   // first and get global tables
-  DArr<uint32_t> lens, slens, sids;
-  HM_TRY(lens.alloc(ctx, n));
-  HM_TRY(slens.alloc(ctx, n));
+  DArr<uint64_t> keys, skeys;
+  DArr<uint32_t> sids;
+  HM_TRY(keys.alloc(ctx, n));
+  HM_TRY(skeys.alloc(ctx, n));
   HM_TRY(sids.alloc(ctx, n));
-  k_gather_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, lens.p);
+  k_touch_keys<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, rows.gos, rows.rog, keys.p);
   HM_LAUNCH_CHECK();
   {
     size_t tb = 0;
-    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, lens.p, slens.p, d_ids, sids.p, (int64_t)n, 0, 32,
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, keys.p, skeys.p, d_ids, sids.p, (int64_t)n, 0, 64,
                                                       st));
     DArr<uint8_t> tmp;
     HM_TRY(tmp.alloc(ctx, tb));
-    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, lens.p, slens.p, d_ids, sids.p, (int64_t)n, 0, 32,
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, keys.p, skeys.p, d_ids, sids.p, (int64_t)n, 0, 64,
                                                       st));
   }
-  k_count_above<<<grid_for(n, kBlock), kBlock, 0, st>>>(slens.p, n, kRowMax, n_long_d);
+  k_count_long<<<grid_for(n, kBlock), kBlock, 0, st>>>(skeys.p, n, n_long_d);
   HM_LAUNCH_CHECK();
   uint64_t nc = 0;
   unsigned int n_long = 0;
@@ -512,9 +524,11 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   uint64_t gtotal = 0;
   if (n_long) {
     std::vector<uint32_t> hid(n_long), hlen(n_long);
+    std::vector<uint64_t> hkey(n_long);
     HM_CUDA(cudaMemcpyAsync(hid.data(), sids.p, sizeof(uint32_t) * n_long, cudaMemcpyDeviceToHost, st));
-    HM_CUDA(cudaMemcpyAsync(hlen.data(), slens.p, sizeof(uint32_t) * n_long, cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaMemcpyAsync(hkey.data(), skeys.p, sizeof(uint64_t) * n_long, cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n_long; ++i) hlen[i] = (uint32_t)hkey[i];
     for (uint32_t i = 0; i < n_long; ++i) {
       uint32_t sl = 1;
       while (sl < 2 * hlen[i]) sl <<= 1;

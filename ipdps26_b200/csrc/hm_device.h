@@ -146,6 +146,7 @@ struct hm_graph {
   hm::DArr<uint32_t> work;  // centres owning oriented wedges, heaviest first
   uint32_t n_work = 0;
   uint32_t n_work_big = 0;  // the first n_work_big centres have rows longer than the small-table limit
+  uint32_t n_work_mid = 0;  // centres [n_work_big, n_work_mid) have rows longer than the warp-kernel limit
   hm::DArr<unsigned long long> counters;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool ev_ready = false;
@@ -224,6 +225,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
                       const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks);
 int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
                 const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
+int presize_h2h(hm_graph* g);
 
 inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
   uint64_t b = (items + per_block - 1) / per_block;

@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -172,6 +174,7 @@ int build_stores(hm_server* s) {
       int rc = build_h2v(g, st.off.data(), st.mem.data(), n);
       if (rc >= 0) rc = build_v2h(g);
       if (rc >= 0) rc = build_h2h_rows(g);
+      if (rc >= 0) rc = presize_h2h(g);
       if (rc < 0) {
         delete g;
         return rc;
@@ -207,6 +210,7 @@ int build_stores(hm_server* s) {
     int rc = build_h2v(g, off.data(), mem.data(), n);
     if (rc >= 0) rc = build_v2h(g);
     if (rc >= 0) rc = build_h2h_rows(g);
+    if (rc >= 0) rc = presize_h2h(g);
     if (rc < 0) {
       delete g;
       return rc;
@@ -288,6 +292,8 @@ void serve_round(hm_server* s, std::vector<ReqPtr>& batch) {
     rows.push_back(&r);
   }
   if (rows.empty()) return;
+  const bool trace = std::getenv("HM_TRACE") != nullptr;
+  const auto t_prep = std::chrono::steady_clock::now();
   const uint32_t R = (uint32_t)rows.size();
   const uint32_t n_del = (uint32_t)dels.size(), n_ins = (uint32_t)ins_graph.size();
   std::vector<uint64_t> before((size_t)R * 30, 0), after((size_t)R * 30, 0), full((size_t)R * 30, 0);
@@ -334,6 +340,10 @@ void serve_round(hm_server* s, std::vector<ReqPtr>& batch) {
     for (Request* r : rows) finish(s, *r, rc);
     return;
   }
+  if (trace)
+    std::fprintf(stderr, "[hm_trace serve_round] requests=%u deletions=%u insertions=%u queried_slots=%zu device=%.1fms\n",
+                 R, n_del, n_ins, qslots.size(),
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_prep).count());
   // results and host id bookkeeping, request by request
   uint32_t ins_pos = 0;
   for (uint32_t row = 0; row < R; ++row) {

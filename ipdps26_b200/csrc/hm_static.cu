@@ -24,6 +24,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "hm_classes.h"
@@ -45,6 +48,10 @@ constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair 
 // bucketized table (4 blocks per SM, load <= 1/2), longer rows with an
 // 8192-slot table (2 per SM).
 constexpr unsigned kSmallRow = 2048;
+// Rows up to kWarpRow go to the warp-per-centre kernel (a 256-slot table per
+// warp, load <= 1/2).
+constexpr unsigned kWarpRow = 128;
+constexpr unsigned kWarpSlots = 256;
 constexpr uint32_t kEmpty = 0xffffffffu;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -192,14 +199,177 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
   wc[30 + (cc == 2) + 2 * (ea + eb)] += n;
 }
 
-// One block per centre a (the lowest-ranked corner of its triangles). The
-// oriented row N+(a) goes into a shared-memory hash table (load <= 1/4 for
-// rows up to 2048) with each entry's overlap and shared-position mask; each
-// warp takes one b in N+(a) and its lanes probe N+(b). For a centre with at
-// most 64 members, g = |a & b & c| = popc(mask_ab & mask_ac) exactly. Star
-// triangles (all three overlaps 1, the same shared node) are only counted
-// per size category in registers; the others are classified and their four
-// counter updates aggregated across the lanes that share them.
+// The table of one centre's oriented row: bucketized keys (4 per 16-byte
+// bucket), each key's overlap with the centre and shared-position mask (or
+// its row index, for the diagnostic pass). Rows too long for it are searched
+// in global memory instead.
+struct CentreTable {
+  const uint32_t* keys;
+  const uint8_t* sovl;
+  const uint64_t* smask;
+  uint32_t shift, bmask;
+  bool in_smem;
+};
+
+// Fills the table with N+(a), threads t = first, first + stride, ...
+__device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys, uint8_t* sovl,
+                                           uint64_t* smask, uint32_t shift, uint32_t bmask, bool flags,
+                                           unsigned first, unsigned stride) {
+  for (uint32_t i = first; i < ad; i += stride) {
+    const uint32_t key = A.pnbr[ao + i];
+    uint32_t bk = hash_slot(key, shift), h = 0;
+    for (bool done = false; !done; bk = (bk + 1) & bmask)
+      for (uint32_t t = 0; t < 4; ++t)
+        if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
+          h = 4 * bk + t;
+          done = true;
+          break;
+        }
+    smask[h] = flags ? (uint64_t)i : A.pmask[ao + i];  // diagnostics keep the row index
+    sovl[h] = (uint8_t)(A.pos[ao + i] & 0xffu);
+  }
+}
+
+// One whole warp: walks N+(b) for the bi-th entry b of N+(a), probes the
+// centre's table, and adds every triangle {a, b, c} it closes to wc. For a
+// centre with at most 64 members g = |a & b & c| = popc(mask_ab & mask_ac)
+// exactly. Star triangles (all three overlaps 1, the same shared node) are
+// only counted per size category in registers; the others are classified and
+// their four counter updates aggregated across the lanes that share them.
+__device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t a, uint32_t sa, uint64_t ao,
+                                                  uint32_t ad, uint32_t bi, const CentreTable& T,
+                                                  unsigned long long* wc, uint32_t cat_a, bool exact_masks,
+                                                  bool flags) {
+  const unsigned lane = lane_id();
+  const uint32_t b = A.pnbr[ao + bi];
+  const uint32_t osb = A.pos[ao + bi];
+  const uint32_t cab = osb & 0xffu, sb = osb >> 8;
+  const uint64_t mab = A.pmask[ao + bi];
+  const uint64_t bo = A.poff[b];
+  const uint32_t bd = A.plen[b];
+  uint32_t star0 = 0, star1 = 0, star2 = 0;
+  // kUnroll probes per lane per round: their id and overlap/size loads are
+  // issued together so several global loads are in flight per lane.
+  for (uint32_t j0 = 0; j0 < bd; j0 += kWarp * kUnroll) {
+    uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      const uint32_t j = j0 + u * kWarp + lane;
+      cv[u] = kEmpty;
+      ov[u] = 0;
+      if (j < bd) {
+        cv[u] = __ldg(A.pnbr + bo + j);
+        ov[u] = __ldg(A.pos + bo + j);
+      }
+    }
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      const uint32_t c = cv[u];
+      if (c == kEmpty) continue;
+      uint32_t cac = 0;
+      uint64_t mac = 0;
+      if (T.in_smem) {
+        uint32_t bk = hash_slot(c, T.shift);
+        int t;
+        for (;;) {
+          const uint4 q = reinterpret_cast<const uint4*>(T.keys)[bk];
+          t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
+          if (t >= 0 || q.w == kEmpty) break;
+          bk = (bk + 1) & T.bmask;
+        }
+        if (t >= 0) {
+          const uint32_t h = 4 * bk + (uint32_t)t;
+          cac = T.sovl[h];
+          mac = T.smask[h];
+          if (flags) {
+            const uint32_t j = j0 + u * kWarp + lane;
+            A.edge_flags[ao + mac] = 1;
+            A.edge_flags[ao + bi] = 1;
+            A.edge_flags[bo + j] = 1;
+            mac = A.pmask[ao + mac];
+          }
+        }
+      } else {
+        uint32_t lo = 0, hi = ad;
+        const uint32_t* row = A.pnbr + ao;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (row[mid] < c) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo < ad && row[lo] == c) {
+          cac = A.pos[ao + lo] & 0xffu;
+          mac = A.pmask[ao + lo];
+          if (flags) {
+            const uint32_t j = j0 + u * kWarp + lane;
+            A.edge_flags[ao + lo] = 1;
+            A.edge_flags[ao + bi] = 1;
+            A.edge_flags[bo + j] = 1;
+          }
+        }
+      }
+      if (!cac) continue;
+      const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
+      uint32_t g;
+      if (exact_masks) {
+        if ((cab | cac | cbc) == 1 && mab == mac) {
+          const uint32_t cc = size_cat(sc);
+          star0 += cc == 0;
+          star1 += cc == 1;
+          star2 += cc == 2;
+          continue;
+        }
+        g = __popcll(mab & mac);
+      } else {
+        g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
+      }
+      const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
+      if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+      // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
+      const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
+      const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
+      const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
+      const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
+      const unsigned peers = __match_any_sync(__activemask(), key);
+      if (lane == (unsigned)(__ffs(peers) - 1)) {
+        const unsigned long long n = (unsigned long long)__popc(peers);
+        atomicAdd(&wc[k], n);
+        atomicAdd(&wc[30 + oa], n);
+        atomicAdd(&wc[30 + ob], n);
+        atomicAdd(&wc[30 + oc], n);
+      }
+    }
+  }
+  if (cab == 1 && exact_masks) {
+    for (int d = 16; d; d >>= 1) {
+      star0 += __shfl_xor_sync(0xffffffffu, star0, d);
+      star1 += __shfl_xor_sync(0xffffffffu, star1, d);
+      star2 += __shfl_xor_sync(0xffffffffu, star2, d);
+    }
+    if (lane == 0) {
+      const uint32_t cat_b = size_cat(sb);
+      if (star0) add_star(wc, cat_a, cat_b, 0, star0);
+      if (star1) add_star(wc, cat_a, cat_b, 1, star1);
+      if (star2) add_star(wc, cat_a, cat_b, 2, star2);
+    }
+  }
+}
+
+// Adds one warp's counters to output row `row` and clears them.
+__device__ __forceinline__ void flush_counts(unsigned long long* wc, unsigned long long* out) {
+  for (unsigned k = lane_id(); k < kNumCounters; k += kWarp)
+    if (wc[k]) {
+      atomicAdd(&out[k], wc[k]);
+      wc[k] = 0;
+    }
+  __syncwarp();
+}
+
+constexpr uint32_t kNoRow = 0xffffffffu;
+
+// One block per centre a (the lowest-ranked corner of its triangles): N+(a)
+// in a shared-memory table (load <= 1/4 up to kHashSlotsMax / 2 entries,
+// else searched in global memory), each warp takes one b in N+(a) at a time.
 template <unsigned kHashSlotsMax, unsigned kMinBlocks>
 __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
   static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
@@ -213,6 +383,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
   for (unsigned k = lane; k < kNumCounters; k += kWarp) wc[k] = 0;
+  uint32_t cur_row = kNoRow;  // per-request rows: the row wc is collecting for
 
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1u);
@@ -220,177 +391,104 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint64_t item = (uint64_t)s_item * A.n_shards + A.shard;
     if (item >= A.n_work) break;
     const uint32_t a = A.work[item];
+    if (A.gos) {
+      const uint32_t row = A.rog[A.gos[a]];
+      if (row != cur_row) {
+        if (cur_row != kNoRow) flush_counts(wc, A.out + (size_t)cur_row * kRowStride);
+        cur_row = row;
+      }
+    }
     const uint64_t ao = A.poff[a];
     const uint32_t ad = A.plen[a];
     const uint32_t sa = A.esize[a];
-    const bool in_smem = ad <= kHashRowMax;
     const bool flags = A.edge_flags != nullptr;
-    // Bucketized table: 4 keys per 16-byte bucket, filled in order, so one
-    // vector load answers a lookup unless the bucket is full (rare at load
-    // factors <= 1/2).
-    uint32_t shift = 32, bmask = 0;
-    if (in_smem) {
+    CentreTable T{keys, sovl, smask, 32, 0, ad <= kHashRowMax};
+    if (T.in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
       const uint32_t buckets = slots / 4;
-      shift = 32 - (31 - __clz(buckets));
-      bmask = buckets - 1;
+      T.shift = 32 - (31 - __clz(buckets));
+      T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      for (uint32_t i = threadIdx.x; i < ad; i += blockDim.x) {
-        const uint32_t key = A.pnbr[ao + i];
-        uint32_t bk = hash_slot(key, shift), h = 0;
-        for (bool done = false; !done; bk = (bk + 1) & bmask)
-          for (uint32_t t = 0; t < 4; ++t)
-            if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
-              h = 4 * bk + t;
-              done = true;
-              break;
-            }
-        smask[h] = flags ? (uint64_t)i : A.pmask[ao + i];  // diagnostics keep the row index
-        sovl[h] = (uint8_t)(A.pos[ao + i] & 0xffu);
-      }
+      fill_table(A, ao, ad, keys, sovl, smask, T.shift, T.bmask, flags, threadIdx.x, blockDim.x);
     }
     __syncthreads();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
     for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
-      const uint32_t b = A.pnbr[ao + bi];
-      const uint32_t osb = A.pos[ao + bi];
-      const uint32_t cab = osb & 0xffu, sb = osb >> 8;
-      const uint64_t mab = A.pmask[ao + bi];
-      const uint64_t bo = A.poff[b];
-      const uint32_t bd = A.plen[b];
-      uint32_t star0 = 0, star1 = 0, star2 = 0;
-      // kUnroll probes per lane per round: their id and overlap/size loads are
-      // issued together so several global loads are in flight per lane.
-      for (uint32_t j0 = 0; j0 < bd; j0 += kWarp * kUnroll) {
-        uint32_t cv[kUnroll], ov[kUnroll];
-#pragma unroll
-        for (unsigned u = 0; u < kUnroll; ++u) {
-          const uint32_t j = j0 + u * kWarp + lane;
-          cv[u] = kEmpty;
-          ov[u] = 0;
-          if (j < bd) {
-            cv[u] = __ldg(A.pnbr + bo + j);
-            ov[u] = __ldg(A.pos + bo + j);
-          }
-        }
-#pragma unroll
-        for (unsigned u = 0; u < kUnroll; ++u) {
-          const uint32_t c = cv[u];
-          if (c == kEmpty) continue;
-          uint32_t cac = 0;
-          uint64_t mac = 0;
-          if (in_smem) {
-            uint32_t bk = hash_slot(c, shift);
-            int t;
-            for (;;) {
-              const uint4 q = reinterpret_cast<const uint4*>(keys)[bk];
-              t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
-              if (t >= 0 || q.w == kEmpty) break;
-              bk = (bk + 1) & bmask;
-            }
-            if (t >= 0) {
-              const uint32_t h = 4 * bk + (uint32_t)t;
-              cac = sovl[h];
-              mac = smask[h];
-              if (flags) {
-                const uint32_t j = j0 + u * kWarp + lane;
-                A.edge_flags[ao + mac] = 1;
-                A.edge_flags[ao + bi] = 1;
-                A.edge_flags[bo + j] = 1;
-                mac = A.pmask[ao + mac];
-              }
-            }
-          } else {
-            uint32_t lo = 0, hi = ad;
-            const uint32_t* row = A.pnbr + ao;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (row[mid] < c) lo = mid + 1;
-              else hi = mid;
-            }
-            if (lo < ad && row[lo] == c) {
-              cac = A.pos[ao + lo] & 0xffu;
-              mac = A.pmask[ao + lo];
-              if (flags) {
-                const uint32_t j = j0 + u * kWarp + lane;
-                A.edge_flags[ao + lo] = 1;
-                A.edge_flags[ao + bi] = 1;
-                A.edge_flags[bo + j] = 1;
-              }
-            }
-          }
-          if (!cac) continue;
-          const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
-          uint32_t g;
-          if (exact_masks) {
-            if ((cab | cac | cbc) == 1 && mab == mac) {
-              const uint32_t cc = size_cat(sc);
-              star0 += cc == 0;
-              star1 += cc == 1;
-              star2 += cc == 2;
-              continue;
-            }
-            g = __popcll(mab & mac);
-          } else {
-            g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
-          }
-          const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
-          if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-          // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
-          const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
-          const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
-          const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
-          const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
-          const unsigned peers = __match_any_sync(__activemask(), key);
-          if (lane == (unsigned)(__ffs(peers) - 1)) {
-            const unsigned long long n = (unsigned long long)__popc(peers);
-            atomicAdd(&wc[k], n);
-            atomicAdd(&wc[30 + oa], n);
-            atomicAdd(&wc[30 + ob], n);
-            atomicAdd(&wc[30 + oc], n);
-          }
-        }
-      }
-      if (cab == 1 && exact_masks) {
-        for (int d = 16; d; d >>= 1) {
-          star0 += __shfl_xor_sync(0xffffffffu, star0, d);
-          star1 += __shfl_xor_sync(0xffffffffu, star1, d);
-          star2 += __shfl_xor_sync(0xffffffffu, star2, d);
-        }
-        if (lane == 0) {
-          const uint32_t cat_b = size_cat(sb);
-          if (star0) add_star(wc, cat_a, cat_b, 0, star0);
-          if (star1) add_star(wc, cat_a, cat_b, 1, star1);
-          if (star2) add_star(wc, cat_a, cat_b, 2, star2);
-        }
-      }
-      __syncwarp();
-    }
-    if (A.gos) {  // per-request rows: this centre's triangles go to its graph's row
-      unsigned long long* o = A.out + (size_t)A.rog[A.gos[a]] * kRowStride;
-      for (unsigned k = lane; k < kNumCounters; k += kWarp)
-        if (wc[k]) {
-          atomicAdd(&o[k], wc[k]);
-          wc[k] = 0;
-        }
+      closed_pairs_of_b(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
       __syncwarp();
     }
     __syncthreads();
   }
   __syncwarp();
-  for (unsigned k = lane; k < kNumCounters; k += kWarp)
-    if (wc[k]) atomicAdd(&A.out[k], wc[k]);
+  flush_counts(wc, A.out + (cur_row == kNoRow ? 0 : (size_t)cur_row * kRowStride));
+}
+
+// One warp per centre, for short oriented rows (<= kWarpRow): each warp
+// holds its own table (load <= 1/2) and walks all of N+(a) itself, with no
+// block-wide barriers; warps take centres from the queue one at a time.
+__global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
+  __shared__ __align__(16) uint32_t keys_all[kClosedWarps][kWarpSlots];
+  __shared__ uint64_t mask_all[kClosedWarps][kWarpSlots];
+  __shared__ uint8_t ovl_all[kClosedWarps][kWarpSlots];
+  __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  uint32_t* keys = keys_all[w];
+  uint64_t* smask = mask_all[w];
+  uint8_t* sovl = ovl_all[w];
+  unsigned long long* wc = wcnt[w];
+  for (unsigned k = lane; k < kNumCounters; k += kWarp) wc[k] = 0;
+  __syncwarp();
+  uint32_t cur_row = kNoRow;
+  const bool flags = A.edge_flags != nullptr;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(A.queue, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    const uint64_t item = (uint64_t)it * A.n_shards + A.shard;
+    if (item >= A.n_work) break;
+    const uint32_t a = A.work[item];
+    if (A.gos) {
+      const uint32_t row = A.rog[A.gos[a]];
+      if (row != cur_row) {
+        if (cur_row != kNoRow) flush_counts(wc, A.out + (size_t)cur_row * kRowStride);
+        cur_row = row;
+      }
+    }
+    const uint64_t ao = A.poff[a];
+    const uint32_t ad = A.plen[a];  // <= kWarpRow by the work split
+    const uint32_t sa = A.esize[a];
+    uint32_t slots = 64;
+    while (slots < 2 * ad && slots < kWarpSlots) slots <<= 1;
+    const uint32_t buckets = slots / 4;
+    CentreTable T{keys, sovl, smask, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true};
+    for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
+    __syncwarp();
+    fill_table(A, ao, ad, keys, sovl, smask, T.shift, T.bmask, flags, lane, kWarp);
+    __syncwarp();
+    const uint32_t cat_a = size_cat(sa);
+    const bool exact_masks = sa <= 64;
+    for (uint32_t bi = 0; bi < ad; ++bi) {
+      closed_pairs_of_b(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  flush_counts(wc, A.out + (cur_row == kNoRow ? 0 : (size_t)cur_row * kRowStride));
 }
 
 // Work estimate per centre: sum of d+(b) over b in N+(a); centres with fewer
-// than two oriented neighbours own no triangle and are dropped (key 0). Rows
-// longer than kSmallRow get the top bit so they sort first and go to the
-// large-table launch.
+// than two oriented neighbours own no triangle and are dropped (key 0). Key
+// layout: bit 63 = row longer than kSmallRow (large-table launch), bit 62 =
+// row longer than kWarpRow (block launch), then the estimate; descending
+// order gives the three launches' lists, heaviest first. With gos set
+// (per-request rows of a pooled store) bits 40..61 hold the output row of the
+// centre's graph above a 40-bit estimate, so that the blocks running at one
+// time share one graph's rows in L2.
 __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, const uint32_t* rows,
-                              uint32_t n, uint64_t* est, uint32_t* ids) {
+                              uint32_t n, const uint32_t* gos, const uint32_t* rog, uint64_t* est, uint32_t* ids) {
   for (uint64_t r = global_warp(); r < n; r += n_warps()) {
     const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint32_t d = plen[a];
@@ -399,8 +497,16 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
       for (uint32_t i = lane_id(); i < d; i += kWarp) s += plen[pnbr[poff[a] + i]];
     s = warp_sum(s);
     if (lane_id() == 0) {
-      uint64_t key = (d >= 2 && s > 0) ? s + d : 0;
-      if (key && d > kSmallRow) key |= 1ull << 63;
+      uint64_t key = 0;
+      if (d >= 2 && s > 0) {
+        const uint64_t e = s + d;
+        if (gos)
+          key = ((uint64_t)min(rog[gos[a]], (1u << 22) - 1u) << 40) | (e < (1ull << 40) ? e : (1ull << 40) - 1);
+        else
+          key = e < (1ull << 62) ? e : (1ull << 62) - 1;
+        if (d > kWarpRow) key |= 1ull << 62;
+        if (d > kSmallRow) key |= 1ull << 63;
+      }
       est[r] = key;
       ids[r] = a;
     }
@@ -424,7 +530,7 @@ static int closed_worklist(hm_graph* g) {
   HM_TRY(ids.alloc(ctx, E));
   HM_TRY(g->work.alloc(ctx, E));
   k_closed_work<<<grid_for((uint64_t)E * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p,
-                                                                nullptr, E, est.p, ids.p);
+                                                                nullptr, E, nullptr, nullptr, est.p, ids.p);
   HM_LAUNCH_CHECK();
   size_t tb = 0;
   HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, g->work.p, (int64_t)E,
@@ -452,6 +558,13 @@ static int closed_worklist(hm_graph* g) {
     else hi = mid;
   }
   g->n_work_big = lo;
+  hi = g->n_work;  // rows longer than kWarpRow carry bit 62 (the big ones too)
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if ((h[mid] >> 62) & 1u) lo = mid + 1;
+    else hi = mid;
+  }
+  g->n_work_mid = lo;
   g->work_valid = true;
   return HM_OK;
 }
@@ -484,15 +597,44 @@ int prepare_static(hm_graph* g) {
   return prepare_static_attrs();
 }
 
+// The closed phase over a work list split at bounds[0..3]: rows longer than
+// kSmallRow (8192-slot tables, 2 blocks per SM), rows longer than kWarpRow
+// (4096-slot tables, 4 blocks per SM), then the short rows, one warp each.
+// queues holds three zeroed counters, one per launch.
+static int launch_closed(hm_ctx* ctx, ClosedArgs base, const uint32_t bounds[4], unsigned int* queues) {
+  cudaStream_t st = ctx->stream;
+  for (int part = 0; part < 3; ++part) {
+    const uint32_t n = bounds[part + 1] - bounds[part];
+    if (n <= base.shard) continue;
+    ClosedArgs A = base;
+    A.work = base.work + bounds[part];
+    A.n_work = n;
+    A.queue = queues + part;
+    const uint32_t items = (n - base.shard + base.n_shards - 1) / base.n_shards;
+    if (part == 0) {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
+      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
+    } else if (part == 1) {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, items);
+      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
+    } else {
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, (items + kClosedWarps - 1) / kClosedWarps);
+      k_closed_warp<<<grid, kClosedBlock, 0, st>>>(A);
+    }
+    HM_LAUNCH_CHECK();
+  }
+  return HM_OK;
+}
+
 // Launches both phases for one shard of the centres; the counters land in
 // g->counters ([0,30) closed classes, [30,36) open-pair removals, [36,42)
-// open-pair counts, [42..43] work queues). edge_flags is for diagnostics.
+// open-pair counts, [42..44] work queues). edge_flags is for diagnostics.
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
-  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 44, st));
+  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 48, st));
   HM_CUDA(cudaEventRecord(g->ev[0], st));
   if (E) {
     k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
@@ -501,25 +643,11 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
     HM_LAUNCH_CHECK();
   }
   HM_CUDA(cudaEventRecord(g->ev[1], st));
-  // rows longer than kSmallRow first (8192-slot tables, 2 blocks per SM),
-  // then the rest (4096-slot tables, 4 blocks per SM)
-  for (int part = 0; part < 2; ++part) {
-    const uint32_t begin = part ? g->n_work_big : 0, end = part ? g->n_work : g->n_work_big;
-    const uint32_t n = end - begin;
-    if (n <= shard) continue;
-    ClosedArgs A{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p,
-                 g->esize.p, g->work.p + begin, n, shard, n_shards,
-                 reinterpret_cast<unsigned int*>(dev + 42 + part), dev, edge_flags, nullptr, nullptr};
-    const uint32_t items = (n - shard + n_shards - 1) / n_shards;
-    if (part == 0) {
-      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
-      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
-    } else {
-      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, items);
-      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
-    }
-    HM_LAUNCH_CHECK();
-  }
+  const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
+  HM_TRY(launch_closed(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
+                                       g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->work.p, 0, shard, n_shards, nullptr,
+                                       dev, edge_flags, nullptr, nullptr},
+                       bounds, reinterpret_cast<unsigned int*>(dev + 42)));
   HM_CUDA(cudaEventRecord(g->ev[2], st));
   return HM_OK;
 }
@@ -546,10 +674,11 @@ int finish_static(hm_graph* g, uint64_t out30[30]) {
 }
 
 namespace {
-__global__ void k_count_work(const uint64_t* est, uint32_t n, unsigned int* out2) {
+__global__ void k_count_work(const uint64_t* est, uint32_t n, unsigned int* out3) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    if (est[i]) atomicAdd(&out2[0], 1u);
-    if (est[i] >> 63) atomicAdd(&out2[1], 1u);
+    if (est[i]) atomicAdd(&out3[0], 1u);
+    if (est[i] >> 63) atomicAdd(&out3[1], 1u);
+    if ((est[i] >> 62) & 1u) atomicAdd(&out3[2], 1u);
   }
 }
 }  // namespace
@@ -564,13 +693,14 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   const uint32_t R = rows.n_rows;
   for (size_t k = 0; k < (size_t)R * 30; ++k) out[k] = 0;
   if (!n) return HM_OK;
+  const auto t_begin = std::chrono::steady_clock::now();
   HM_TRY(prepare_static_attrs());
   PlusRows P;
   HM_TRY(build_plus_rows(g, d_rows, n, &P));
   DArr<uint64_t> est, est_sorted;
   DArr<uint32_t> ids, work;
   DArr<unsigned long long> cnt;
-  const size_t n_cnt = (size_t)R * kRowStride + 4;  // + two queues, + two work counts
+  const size_t n_cnt = (size_t)R * kRowStride + 5;  // + three queues, + three work counts
   HM_TRY(est.alloc(ctx, n));
   HM_TRY(est_sorted.alloc(ctx, n));
   HM_TRY(ids.alloc(ctx, n));
@@ -578,7 +708,8 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   HM_TRY(cnt.alloc(ctx, n_cnt));
   HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * n_cnt, st));
   unsigned long long* tail = cnt.p + (size_t)R * kRowStride;
-  k_closed_work<<<grid_for((uint64_t)n * 32, 256), 256, 0, st>>>(P.off.p, P.len.p, P.nbr.p, d_rows, n, est.p, ids.p);
+  k_closed_work<<<grid_for((uint64_t)n * 32, 256), 256, 0, st>>>(P.off.p, P.len.p, P.nbr.p, d_rows, n, rows.gos,
+                                                                rows.rog, est.p, ids.p);
   HM_LAUNCH_CHECK();
   {
     size_t tb = 0;
@@ -589,36 +720,28 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
     HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, est.p, est_sorted.p, ids.p, work.p, (int64_t)n, 0,
                                                       64, st));
   }
-  unsigned int* wc = reinterpret_cast<unsigned int*>(tail + 2);
+  unsigned int* wc = reinterpret_cast<unsigned int*>(tail + 3);
   k_count_work<<<grid_for(n, 256), 256, 0, st>>>(est_sorted.p, n, wc);
   HM_LAUNCH_CHECK();
   k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
                                                                g->h2h_ovl.p, g->esize.p, d_rows, n, 0, 1, rows.gos,
                                                                rows.rog, cnt.p + 36);
   HM_LAUNCH_CHECK();
-  unsigned int hw[2] = {0, 0};
+  unsigned int hw[3] = {0, 0, 0};
   HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
   const uint32_t n_work = hw[0], n_big = hw[1];
-  for (int part = 0; part < 2; ++part) {
-    const uint32_t begin = part ? n_big : 0, end = part ? n_work : n_big;
-    const uint32_t m = end - begin;
-    if (!m) continue;
-    ClosedArgs A{P.off.p, P.len.p, P.nbr.p, P.os.p, P.mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p,
-                 work.p + begin, m, 0, 1, reinterpret_cast<unsigned int*>(tail + part), cnt.p, nullptr, rows.gos,
-                 rows.rog};
-    if (part == 0) {
-      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, m);
-      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
-    } else {
-      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, m);
-      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
-    }
-    HM_LAUNCH_CHECK();
-  }
+  const uint32_t bounds[4] = {0, n_big, hw[2], n_work};
+  HM_TRY(launch_closed(ctx, ClosedArgs{P.off.p, P.len.p, P.nbr.p, P.os.p, P.mask.p, g->h2v_off.p, g->h2v_mem.p,
+                                       g->esize.p, work.p, 0, 0, 1, nullptr, cnt.p, nullptr, rows.gos, rows.rog},
+                       bounds, reinterpret_cast<unsigned int*>(tail)));
   std::vector<unsigned long long> h((size_t)R * kRowStride);
   HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
+  if (std::getenv("HM_TRACE"))
+    std::fprintf(stderr, "[hm_trace static_rows] rows=%u oriented=%llu work=%u big=%u total=%.1fms\n", n,
+                 (unsigned long long)P.nnz, n_work, n_big,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count());
   for (uint32_t r = 0; r < R; ++r) {
     const unsigned long long* x = h.data() + (size_t)r * kRowStride;
     uint64_t* o = out + (size_t)r * 30;
