@@ -104,6 +104,23 @@ int hm_gen_batch(const hm_gen_params* p, uint64_t batch_seed, const uint32_t* li
 int hm_hostgraph_view(const hm_hostgraph* hg, hm_hostgraph_info* info);
 void hm_hostgraph_free(hm_hostgraph* hg);
 
+/* Files in the reference programs' formats.
+ *   HM_FMT_ESCHER: space-separated vertex ids >= 1 per line, '#' comments
+ *     (dynamicHyperGraph/utils/utils.cpp:88-130 loadHypergraphFromFile; vertex
+ *     v is node v - 1);
+ *   HM_FMT_MOCHY: comma-separated node ids >= 0 per line
+ *     (MoCHy-master/read_data.cpp:8-45; repeated ids in a line count once);
+ *   HM_FMT_THYME: "n1,n2,...<TAB>time" (THyMe-main/code/read_data.cpp:22-57;
+ *     times must be integers).
+ * A graph read from a file has n_nodes = largest node id + 1. */
+#define HM_FMT_ESCHER 0
+#define HM_FMT_MOCHY 1
+#define HM_FMT_THYME 2
+int hm_hostgraph_read(const char* path, int format, hm_hostgraph** out);
+int hm_hostgraph_write(const hm_hostgraph* hg, const char* path, int format);
+int hm_hostgraph_from_csr(const uint64_t* offsets, const uint32_t* members, uint32_t n_edges, uint32_t n_nodes,
+                          const int64_t* times, hm_hostgraph** out);
+
 /* ---- contexts --------------------------------------------------------- */
 typedef struct hm_ctx hm_ctx;
 typedef struct hm_graph hm_graph;
@@ -266,6 +283,48 @@ int hm_graph_timings(const hm_graph* g, hm_timings_t* t);
  * of x, y, z; x&y only; y&z only; z&x only; x&y&z. */
 int hm_classify_static(int pattern);
 int hm_classify_temporal(int pattern);
+
+/* The reference's vertex-triad counts (temporalDynamicHMotif/src/type1.cu,
+ * type2.cu, type3.cu and their host versions type{1,2,3}.cpp):
+ *   out3[0] type 1: sum over hyperedges of C(|e|, 3);
+ *   out3[1] type 2: sum over adjacent pairs i < j with a = |i & j| >= 2 and
+ *           both |i| - a, |j| - a > 0 of C(a, 2) (|i| - a) (|j| - a);
+ *   out3[2] type 3: sum over pairwise-adjacent triples of x y z, x, y, z the
+ *           pairwise overlaps minus the triple overlap, all three > 0. */
+int hm_count_vertex_triads(hm_graph* g, uint64_t out3[3]);
+
+/* ---- Three-layer temporal window, strictly increasing count --------------
+ * Replaces TemporalCBSTOperations / TemporalHypergraphIndex, a 3-slot ring of
+ * stores (temporalDynamicHMotif/include/temporal_structure.hpp:22-80,
+ * include/temporal_adjacency.hpp:9-19), and computeTemporalMotifCountsStrictInc
+ * (include/temporal_count.hpp:10-16, src/temporal_count.cu:91-217): closed
+ * triples (i of Older, j of Middle, k of Newest) with layer-local ids
+ * i < j < k and all pairwise overlaps non-empty, by the 30 static classes,
+ * without the reference's cap of 1024 candidates per middle hyperedge.
+ * Hyperedge ids are 0-based per layer; node ids < n_nodes. */
+typedef struct hm_window hm_window;
+#define HM_LAYER_OLDER 0
+#define HM_LAYER_MIDDLE 1
+#define HM_LAYER_NEWEST 2
+int hm_window_create(hm_ctx* ctx, uint32_t n_nodes, hm_window** out);
+int hm_window_destroy(hm_window* w);
+/* construct(layer, ...): the layer's hyperedges, replacing what it held */
+int hm_window_set_layer(hm_window* w, int layer, const uint64_t* offsets, const uint32_t* members, uint32_t n_edges);
+/* rotate(): Middle becomes Older, Newest Middle, Older Newest (contents kept) */
+int hm_window_rotate(hm_window* w);
+/* resetLayer(layer): the layer becomes empty */
+int hm_window_reset_layer(hm_window* w, int layer);
+/* fill / unfill (fillCBST / unfillCBST): add or remove vertices of existing
+ * hyperedges; prefix[i] is the inclusive end of ids[i]'s values */
+int hm_window_fill(hm_window* w, int layer, const uint32_t* ids, uint32_t n, const uint32_t* values,
+                   const uint64_t* prefix);
+int hm_window_unfill(hm_window* w, int layer, const uint32_t* ids, uint32_t n, const uint32_t* values,
+                     const uint64_t* prefix);
+/* applyTemporalDeltasFromFile: lines "A <hyperedge> v..." / "R <hyperedge> v..."
+ * (1-based ids and vertices) on the Newest layer; removals applied first */
+int hm_window_apply_deltas_file(hm_window* w, const char* path);
+int hm_window_layer_size(const hm_window* w, int layer, uint32_t* n_edges);
+int hm_window_count30(hm_window* w, uint64_t out30[HM_N_STATIC_CLASSES]);
 
 /* ---- Serving: many resident graphs behind one request loop ---------------
  * No reference counterpart: the reference drivers call applyIncrementalUpdates

@@ -93,7 +93,28 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_cli(force)
     return LIB
+
+
+CLI_SRC = PKG / "cli" / "hmotif_cli.cpp"
+CLI = PKG / "hmotif"
+
+
+def build_cli(force: bool = False) -> Path:
+    """The command-line driver: host C++ over the C ABI, linked against
+    libhmotif.so next to it."""
+    if not force and not _stale(CLI, [CLI_SRC, LIB, ROOT / "include" / "hmotif.h"]):
+        return CLI
+    cxx = shutil.which("g++") or "g++"
+    tmp = CLI.with_suffix(".tmp")
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", str(CLI_SRC), "-o", str(tmp),
+           f"-L{PKG}", "-lhmotif", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed on {CLI_SRC.name}:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, CLI)
+    return CLI
 
 
 def main() -> None:

@@ -266,3 +266,10 @@ extern "C" int hm_debug_touch_orientation(hm_graph* g, int by_id) {
   g->touch_by_id = by_id != 0;
   return HM_OK;
 }
+
+extern "C" int hm_count_vertex_triads(hm_graph* g, uint64_t out3[3]) {
+  if (!g || !out3) return hm::set_error(HM_ERR_INVALID, "hm_count_vertex_triads: NULL argument");
+  HM_TRY(static_ok(g));
+  CtxLock lock(g->ctx);
+  return hm::count_vertex_triads(g, out3);
+}

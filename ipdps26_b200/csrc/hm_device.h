@@ -201,6 +201,7 @@ int prepare_static(hm_graph* g);
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags);
 int finish_static(hm_graph* g, uint64_t out30[30]);
 int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
+int count_vertex_triads(hm_graph* g, uint64_t out3[3]);
 
 // Touched-triple counts (hm_delta.cu). With gos set, the triples of each
 // touched hyperedge's graph gos[slot] go to output row rog[gos[slot]]

@@ -145,13 +145,6 @@ struct DedupeSet {
 
 using hm::Rng;
 
-struct hm_hostgraph {
-  std::vector<uint64_t> offsets;
-  std::vector<uint32_t> members;
-  std::vector<int64_t> times;
-  uint32_t n_nodes = 0;
-  uint64_t redraws = 0;
-};
 
 static int check_params(const hm_gen_params* p) {
   if (!p || p->n_nodes == 0 || p->k_min < 1 || p->k_max < p->k_min || p->k_max > HM_MAX_EDGE_SIZE ||

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/hmotif.h"
 
@@ -13,3 +14,13 @@ namespace hm {
 int set_error(int status, const char* fmt, ...);
 
 }  // namespace hm
+
+// A host-side hypergraph (generator output, files read or written).
+struct hm_hostgraph {
+  std::vector<uint64_t> offsets;
+  std::vector<uint32_t> members;
+  std::vector<int64_t> times;
+  uint32_t n_nodes = 0;
+  uint64_t redraws = 0;
+};
+

@@ -236,6 +236,10 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
 // exactly. Star triangles (all three overlaps 1, the same shared node) are
 // only counted per size category in registers; the others are classified and
 // their four counter updates aggregated across the lanes that share them.
+// kTriads: instead of classes, wc[0] collects sum x * y * z over the
+// triangles, x, y, z the pairwise overlaps minus the triple overlap (all > 0;
+// star triangles give 0), the reference's type-3 vertex triads.
+template <bool kTriads>
 __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t a, uint32_t sa, uint64_t ao,
                                                   uint32_t ad, uint32_t bi, const CentreTable& T,
                                                   unsigned long long* wc, uint32_t cat_a, bool exact_masks,
@@ -248,6 +252,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   const uint64_t bo = A.poff[b];
   const uint32_t bd = A.plen[b];
   uint32_t star0 = 0, star1 = 0, star2 = 0;
+  unsigned long long triads = 0;
   // kUnroll probes per lane per round: their id and overlap/size loads are
   // issued together so several global loads are in flight per lane.
   for (uint32_t j0 = 0; j0 < bd; j0 += kWarp * kUnroll) {
@@ -313,15 +318,21 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
       uint32_t g;
       if (exact_masks) {
         if ((cab | cac | cbc) == 1 && mab == mac) {
-          const uint32_t cc = size_cat(sc);
-          star0 += cc == 0;
-          star1 += cc == 1;
-          star2 += cc == 2;
+          if (!kTriads) {
+            const uint32_t cc = size_cat(sc);
+            star0 += cc == 0;
+            star1 += cc == 1;
+            star2 += cc == 2;
+          }
           continue;
         }
         g = __popcll(mab & mac);
       } else {
         g = triple_overlap(A.hoff, A.hmem, A.esize, a, b, c);
+      }
+      if (kTriads) {
+        if (cab > g && cbc > g && cac > g) triads += (unsigned long long)(cab - g) * (cbc - g) * (cac - g);
+        continue;
       }
       const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
       if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
@@ -339,6 +350,11 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
         atomicAdd(&wc[30 + oc], n);
       }
     }
+  }
+  if (kTriads) {
+    for (int d = 16; d; d >>= 1) triads += __shfl_xor_sync(0xffffffffu, triads, d);
+    if (lane == 0 && triads) wc[0] += triads;
+    return;
   }
   if (cab == 1 && exact_masks) {
     for (int d = 16; d; d >>= 1) {
@@ -370,7 +386,7 @@ constexpr uint32_t kNoRow = 0xffffffffu;
 // One block per centre a (the lowest-ranked corner of its triangles): N+(a)
 // in a shared-memory table (load <= 1/4 up to kHashSlotsMax / 2 entries,
 // else searched in global memory), each warp takes one b in N+(a) at a time.
-template <unsigned kHashSlotsMax, unsigned kMinBlocks>
+template <unsigned kHashSlotsMax, unsigned kMinBlocks, bool kTriads = false>
 __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
   static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
   constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
@@ -417,7 +433,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
     for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
-      closed_pairs_of_b(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
+      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
       __syncwarp();
     }
     __syncthreads();
@@ -429,6 +445,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
 // One warp per centre, for short oriented rows (<= kWarpRow): each warp
 // holds its own table (load <= 1/2) and walks all of N+(a) itself, with no
 // block-wide barriers; warps take centres from the queue one at a time.
+template <bool kTriads = false>
 __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
   __shared__ __align__(16) uint32_t keys_all[kClosedWarps][kWarpSlots];
   __shared__ uint64_t mask_all[kClosedWarps][kWarpSlots];
@@ -471,7 +488,7 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
     for (uint32_t bi = 0; bi < ad; ++bi) {
-      closed_pairs_of_b(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
+      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
       __syncwarp();
     }
   }
@@ -576,6 +593,10 @@ static int prepare_static_attrs() {
                                  (int)closed_smem_bytes(kBigSlots)));
     HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)closed_smem_bytes(kSmallSlots)));
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kBigSlots)));
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)closed_smem_bytes(kSmallSlots)));
     attr_set = true;
   }
   return HM_OK;
@@ -601,6 +622,7 @@ int prepare_static(hm_graph* g) {
 // kSmallRow (8192-slot tables, 2 blocks per SM), rows longer than kWarpRow
 // (4096-slot tables, 4 blocks per SM), then the short rows, one warp each.
 // queues holds three zeroed counters, one per launch.
+template <bool kTriads = false>
 static int launch_closed(hm_ctx* ctx, ClosedArgs base, const uint32_t bounds[4], unsigned int* queues) {
   cudaStream_t st = ctx->stream;
   for (int part = 0; part < 3; ++part) {
@@ -613,13 +635,13 @@ static int launch_closed(hm_ctx* ctx, ClosedArgs base, const uint32_t bounds[4],
     const uint32_t items = (n - base.shard + base.n_shards - 1) / base.n_shards;
     if (part == 0) {
       const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
-      k_closed<kBigSlots, 2><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
+      k_closed<kBigSlots, 2, kTriads><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
     } else if (part == 1) {
       const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, items);
-      k_closed<kSmallSlots, 4><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
+      k_closed<kSmallSlots, 4, kTriads><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
     } else {
       const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, (items + kClosedWarps - 1) / kClosedWarps);
-      k_closed_warp<<<grid, kClosedBlock, 0, st>>>(A);
+      k_closed_warp<kTriads><<<grid, kClosedBlock, 0, st>>>(A);
     }
     HM_LAUNCH_CHECK();
   }
@@ -748,6 +770,61 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
     for (int k = 0; k < 30; ++k) o[k] = x[k];
     for (int k = 0; k < 6; ++k) o[20 + k] += x[36 + k] - x[30 + k];
   }
+  return HM_OK;
+}
+
+namespace {
+// type 1 (sum of C(|a|, 3)) and type 2 (adjacent pairs a < b with overlap
+// o >= 2: C(o, 2) (|a| - o) (|b| - o)); one warp per slot.
+__global__ void k_triads12(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint8_t* ovl,
+                           const uint8_t* esize, uint32_t n, unsigned long long* out2) {
+  unsigned long long t1 = 0, t2 = 0;
+  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+    const uint64_t sa = esize[a];
+    if (lane_id() == 0 && sa >= 3) t1 += sa * (sa - 1) * (sa - 2) / 6;
+    const uint64_t o0 = off[a];
+    for (uint32_t i = lane_id(); i < len[a]; i += kWarp) {
+      const uint32_t b = nbr[o0 + i];
+      const uint64_t o = ovl[o0 + i], sb = esize[b];
+      if (b > a && o >= 2 && sa > o && sb > o) t2 += o * (o - 1) / 2 * (sa - o) * (sb - o);
+    }
+  }
+  t1 = warp_sum(t1);
+  t2 = warp_sum(t2);
+  if (lane_id() == 0) {
+    if (t1) atomicAdd(&out2[0], t1);
+    if (t2) atomicAdd(&out2[1], t2);
+  }
+}
+}  // namespace
+
+// The reference's three vertex-triad counts (temporalDynamicHMotif/src/
+// type1.cu:27-47, type2.cu:47-86, type3.cu:61-122): type 1 and 2 from the
+// sizes and the adjacency, type 3 from one pass of the closed-triangle
+// kernels in their triad mode.
+int count_vertex_triads(hm_graph* g, uint64_t out3[3]) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  HM_TRY(prepare_static(g));
+  DArr<unsigned long long> cnt;
+  HM_TRY(cnt.alloc(ctx, 8));  // [0] type 3, [1..3] queues, [4] type 1, [5] type 2
+  HM_CUDA(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), st));
+  if (g->n_slots) {
+    k_triads12<<<(unsigned)ctx->n_sms * 8, 256, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p,
+                                                         g->esize.p, g->n_slots, cnt.p + 4);
+    HM_LAUNCH_CHECK();
+  }
+  const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
+  HM_TRY(launch_closed<true>(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
+                                             g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->work.p, 0,
+                                             0, 1, nullptr, cnt.p, nullptr, nullptr, nullptr},
+                             bounds, reinterpret_cast<unsigned int*>(cnt.p + 1)));
+  unsigned long long h[8];
+  HM_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  out3[0] = h[4];
+  out3[1] = h[5];
+  out3[2] = h[0];
   return HM_OK;
 }
 

@@ -117,6 +117,7 @@ _lib.bind(
         "hm_count_touching30": (C.c_int, [vp, u32p, C.c_uint32, u64p]),
         "hm_count_temporal": (C.c_int, [vp, C.c_int64, u64p]),
         "hm_debug_touch_orientation": (C.c_int, [vp, C.c_int]),
+        "hm_count_vertex_triads": (C.c_int, [vp, u64p]),
         "hm_serve_create": (C.c_int, [vp, C.POINTER(ServeConfig), C.POINTER(vp)]),
         "hm_serve_add_graph": (C.c_int, [vp, u64p, u32p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_serve_start": (C.c_int, [vp]),
@@ -128,6 +129,16 @@ _lib.bind(
         "hm_serve_stats": (C.c_int, [vp, C.POINTER(ServeStats)]),
         "hm_serve_live_ids": (C.c_int, [vp, C.c_uint32, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_serve_destroy": (C.c_int, [vp]),
+        "hm_window_create": (C.c_int, [vp, C.c_uint32, C.POINTER(vp)]),
+        "hm_window_destroy": (C.c_int, [vp]),
+        "hm_window_set_layer": (C.c_int, [vp, C.c_int, u64p, u32p, C.c_uint32]),
+        "hm_window_rotate": (C.c_int, [vp]),
+        "hm_window_reset_layer": (C.c_int, [vp, C.c_int]),
+        "hm_window_fill": (C.c_int, [vp, C.c_int, u32p, C.c_uint32, u32p, u64p]),
+        "hm_window_unfill": (C.c_int, [vp, C.c_int, u32p, C.c_uint32, u32p, u64p]),
+        "hm_window_apply_deltas_file": (C.c_int, [vp, C.c_char_p]),
+        "hm_window_layer_size": (C.c_int, [vp, C.c_int, C.POINTER(C.c_uint32)]),
+        "hm_window_count30": (C.c_int, [vp, u64p]),
         "hm_classify_static": (C.c_int, [C.c_int]),
         "hm_classify_temporal": (C.c_int, [C.c_int]),
     }
@@ -267,6 +278,12 @@ class Graph:
               "hm_count_touching30")
         return out
 
+    def count_vertex_triads(self) -> np.ndarray:
+        """The reference's type 1, 2 and 3 vertex-triad counts."""
+        out = np.zeros(3, np.uint64)
+        check(lib.hm_count_vertex_triads(self._h, ptr(out, C.c_uint64)), "hm_count_vertex_triads")
+        return out
+
     def set_touch_orientation(self, by_id: bool) -> None:
         """Walk order of the touched-triple counts (same counts either way)."""
         check(lib.hm_debug_touch_orientation(self._h, int(by_id)), "hm_debug_touch_orientation")
@@ -284,6 +301,78 @@ class Graph:
     def close(self) -> None:
         if self._h:
             lib.hm_graph_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+OLDER, MIDDLE, NEWEST = 0, 1, 2
+
+
+class Window:
+    """Three-layer temporal window (Older, Middle, Newest) and its strictly
+    increasing 30-class count (hm_window_* in hmotif.h)."""
+
+    def __init__(self, ctx: Context, n_nodes: int):
+        h = vp()
+        check(lib.hm_window_create(ctx.handle, int(n_nodes), C.byref(h)), "hm_window_create")
+        self._h = h
+        self.ctx = ctx
+        ctx._children.add(self)
+
+    def set_layer(self, layer: int, offsets, members) -> None:
+        off, mem = _csr_arrays(offsets, members)
+        check(lib.hm_window_set_layer(self._h, layer, ptr(off, C.c_uint64),
+                                      ptr(mem if len(mem) else np.zeros(1, np.uint32), C.c_uint32), len(off) - 1),
+              "hm_window_set_layer")
+
+    def rotate(self) -> None:
+        check(lib.hm_window_rotate(self._h), "hm_window_rotate")
+
+    def reset_layer(self, layer: int) -> None:
+        check(lib.hm_window_reset_layer(self._h, layer), "hm_window_reset_layer")
+
+    def _fill(self, fn, name, layer, ids, values_per_id):
+        ids = np.ascontiguousarray(ids, np.uint32)
+        vals = np.ascontiguousarray(np.concatenate([np.asarray(v, np.uint32) for v in values_per_id])
+                                    if len(values_per_id) else np.zeros(0, np.uint32), np.uint32)
+        pre = np.cumsum([len(v) for v in values_per_id]).astype(np.uint64) if len(values_per_id) else np.zeros(0, np.uint64)
+        check(fn(self._h, layer, ptr(ids if len(ids) else np.zeros(1, np.uint32), C.c_uint32), len(ids),
+                 ptr(vals if len(vals) else np.zeros(1, np.uint32), C.c_uint32),
+                 ptr(pre if len(pre) else np.zeros(1, np.uint64), C.c_uint64)), name)
+
+    def fill(self, layer: int, ids, values_per_id) -> None:
+        self._fill(lib.hm_window_fill, "hm_window_fill", layer, ids, values_per_id)
+
+    def unfill(self, layer: int, ids, values_per_id) -> None:
+        self._fill(lib.hm_window_unfill, "hm_window_unfill", layer, ids, values_per_id)
+
+    def apply_deltas_file(self, path) -> None:
+        check(lib.hm_window_apply_deltas_file(self._h, str(path).encode()), "hm_window_apply_deltas_file")
+
+    def layer_size(self, layer: int) -> int:
+        n = C.c_uint32()
+        check(lib.hm_window_layer_size(self._h, layer, C.byref(n)), "hm_window_layer_size")
+        return n.value
+
+    def count30(self) -> np.ndarray:
+        out = np.zeros(N_STATIC_CLASSES, np.uint64)
+        check(lib.hm_window_count30(self._h, ptr(out, C.c_uint64)), "hm_window_count30")
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib.hm_window_destroy(self._h)
             self._h = None
 
     def __enter__(self):

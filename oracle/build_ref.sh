@@ -7,6 +7,9 @@
 #   MoCHy-master/main_exact_par.cpp   -> _ref/mochy_exact_par   (OpenMP)
 #   THyMe-main/code/main_thyme.cpp    -> _ref/thyme
 #   THyMe-main/code/main_thymeP.cpp   -> _ref/thymeP            (OpenMP)
+#   temporalDynamicHMotif/src/type{1,2,3}.cpp, through the harness
+#   ref_types.cpp (its main renamed), with graphGeneration.cpp and utils/
+#                                     -> _ref/type1, type2, type3
 set -euo pipefail
 REF=${HM_REFERENCE_ROOT:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -22,4 +25,11 @@ $CXX -O3 -std=c++11 -o "$OUT/mochy_exact" "$REF/MoCHy-master/main_exact.cpp"
 $CXX -O3 -std=c++11 -fopenmp -o "$OUT/mochy_exact_par" "$REF/MoCHy-master/main_exact_par.cpp"
 $CXX -O3 -std=c++11 -o "$OUT/thyme" "$REF/THyMe-main/code/main_thyme.cpp"
 $CXX -O3 -std=c++11 -fopenmp -o "$OUT/thymeP" "$REF/THyMe-main/code/main_thymeP.cpp"
+TD="$REF/temporalDynamicHMotif"
+if [ -d "$TD/src" ]; then
+  for t in 1 2 3; do
+    $CXX -O2 -std=c++17 -DHM_TYPE=$t -I"$TD" -o "$OUT/type$t" "$HERE/ref_types.cpp" "$TD/src/graphGeneration.cpp" \
+      "$TD/utils/utils.cpp" "$TD/utils/printUtils.cpp" "$TD/utils/flatten.cpp"
+  done
+fi
 echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"

@@ -326,6 +326,83 @@ int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* memb
   return hmo_static30_shard(n_edges, offsets, members, n_nodes, 0, 1, out30);
 }
 
+/* Strictly increasing three-layer count, restating the reference's
+ * temporalStrictIncAdjKernel (temporalDynamicHMotif/src/temporal_count.cu:
+ * 91-170): closed triples (i of the older layer, j of the middle, k of the
+ * newest) with layer-local ids i < j < k and all three pairwise overlaps
+ * non-empty, by static class of (|i|, |j|, |k|, C_ij, C_jk, C_ik, g). The
+ * reference stops collecting candidates at 1024 per middle hyperedge; this
+ * restatement has no such cap. Brute force over all (i, j, k). */
+int hmo_strictinc30(const uint64_t* off0, const uint32_t* mem0, uint32_t n0, const uint64_t* off1,
+                    const uint32_t* mem1, uint32_t n1, const uint64_t* off2, const uint32_t* mem2, uint32_t n2,
+                    uint64_t out30[30]) {
+  csr_t L0, L1, L2;
+  memset(out30, 0, sizeof(uint64_t) * 30);
+  if (csr_from_input(n0, off0, mem0, &L0)) return -1;
+  if (csr_from_input(n1, off1, mem1, &L1)) { csr_free(&L0); return -1; }
+  if (csr_from_input(n2, off2, mem2, &L2)) { csr_free(&L0); csr_free(&L1); return -1; }
+  for (uint32_t j = 0; j < n1; ++j) {
+    const uint32_t* mj = L1.mem + L1.off[j];
+    const uint32_t sj = (uint32_t)(L1.off[j + 1] - L1.off[j]);
+    for (uint32_t i = 0; i < n0 && i < j; ++i) {
+      const uint32_t* mi = L0.mem + L0.off[i];
+      const uint32_t si = (uint32_t)(L0.off[i + 1] - L0.off[i]);
+      const uint32_t cij = inter_count(mi, si, mj, sj);
+      if (!cij) continue;
+      for (uint32_t k = j + 1; k < n2; ++k) {
+        const uint32_t* mk = L2.mem + L2.off[k];
+        const uint32_t sk = (uint32_t)(L2.off[k + 1] - L2.off[k]);
+        const uint32_t cjk = inter_count(mj, sj, mk, sk);
+        if (!cjk) continue;
+        const uint32_t cik = inter_count(mi, si, mk, sk);
+        if (!cik) continue;
+        const uint32_t g = inter3_count(mi, si, mj, sj, mk, sk);
+        int c = hmo_static_class((int)si, (int)sj, (int)sk, (int)cij, (int)cjk, (int)cik, (int)g);
+        if (c >= 0) out30[c]++;
+      }
+    }
+  }
+  csr_free(&L0);
+  csr_free(&L1);
+  csr_free(&L2);
+  return 0;
+}
+
+/* Vertex-triad counts of the reference's type1/type2/type3 programs
+ * (temporalDynamicHMotif/src/type1.cpp:6-15, type2.cpp:17-44,
+ * type3.cpp:58-94), restated over the deduplicated member lists:
+ *   type1 = sum over hyperedges of C(|e|, 3);
+ *   type2 = sum over adjacent pairs i < j with a = |i & j| >= 2,
+ *           b = |i| - a > 0, c = |j| - a > 0 of C(a, 2) * b * c;
+ *   type3 = sum over pairwise-adjacent i < j < k of x * y * z, x, y, z the
+ *           pairwise overlaps minus the triple overlap, all three > 0. */
+int hmo_vertex_triads(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint64_t out3[3]) {
+  csr_t h;
+  out3[0] = out3[1] = out3[2] = 0;
+  if (csr_from_input(n_edges, offsets, members, &h)) return -1;
+  for (uint32_t i = 0; i < n_edges; ++i) {
+    const uint64_t si = h.off[i + 1] - h.off[i];
+    if (si >= 3) out3[0] += si * (si - 1) * (si - 2) / 6;
+    for (uint32_t j = i + 1; j < n_edges; ++j) {
+      const uint32_t sj = (uint32_t)(h.off[j + 1] - h.off[j]);
+      const uint32_t a = inter_count(h.mem + h.off[i], (uint32_t)si, h.mem + h.off[j], sj);
+      if (!a) continue;
+      if (a >= 2 && si > a && sj > a) out3[1] += (uint64_t)a * (a - 1) / 2 * (si - a) * (sj - a);
+      for (uint32_t k = j + 1; k < n_edges; ++k) {
+        const uint32_t sk = (uint32_t)(h.off[k + 1] - h.off[k]);
+        const uint32_t b = inter_count(h.mem + h.off[j], sj, h.mem + h.off[k], sk);
+        if (!b) continue;
+        const uint32_t c = inter_count(h.mem + h.off[i], (uint32_t)si, h.mem + h.off[k], sk);
+        if (!c) continue;
+        const uint32_t g = inter3_count(h.mem + h.off[i], (uint32_t)si, h.mem + h.off[j], sj, h.mem + h.off[k], sk);
+        if (a > g && b > g && c > g) out3[2] += (uint64_t)(a - g) * (b - g) * (c - g);
+      }
+    }
+  }
+  csr_free(&h);
+  return 0;
+}
+
 /* The 26 reported motifs: classes other than 0, 1, 4, 6
  * (MoCHy-master/main_exact.cpp:133-137). */
 void hmo_static26_from30(const uint64_t in30[30], uint64_t out26[26]) {

@@ -22,6 +22,10 @@ int hmo_static30(uint32_t n_edges, const uint64_t* offsets, const uint32_t* memb
                  uint64_t out30[30]);
 int hmo_static30_shard(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint32_t n_nodes,
                        uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
+int hmo_strictinc30(const uint64_t* off0, const uint32_t* mem0, uint32_t n0, const uint64_t* off1,
+                    const uint32_t* mem1, uint32_t n1, const uint64_t* off2, const uint32_t* mem2, uint32_t n2,
+                    uint64_t out30[30]);
+int hmo_vertex_triads(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint64_t out3[3]);
 void hmo_static26_from30(const uint64_t in30[30], uint64_t out26[26]);
 int hmo_static30_brute(uint32_t n_edges, const uint64_t* offsets, const uint32_t* members, uint64_t out30[30]);
 

@@ -32,6 +32,8 @@ def lib():
         u32p, u64p, i64p = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_int64)
         L.hmo_static30.argtypes = [C.c_uint32, u64p, u32p, C.c_uint32, u64p]
         L.hmo_static30_shard.argtypes = [C.c_uint32, u64p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, u64p]
+        L.hmo_strictinc30.argtypes = [u64p, u32p, C.c_uint32] * 3 + [u64p]
+        L.hmo_vertex_triads.argtypes = [C.c_uint32, u64p, u32p, u64p]
         L.hmo_static30_brute.argtypes = [C.c_uint32, u64p, u32p, u64p]
         L.hmo_temporal96.argtypes = [C.c_uint32, u64p, u32p, i64p, C.c_int64, u64p]
         L.hmo_temporal96_brute.argtypes = [C.c_uint32, u64p, u32p, i64p, C.c_int64, u64p]
@@ -79,6 +81,32 @@ def static30_shard(offsets, members, n_nodes: int, shard: int, n_shards: int) ->
                                   _p(out, C.c_uint64))
     if rc != 0:
         raise RuntimeError(f"hmo_static30_shard failed: {rc}")
+    return out
+
+
+def strictinc30(layers) -> np.ndarray:
+    """Three-layer strictly increasing count; layers = [(offsets, members)] * 3
+    in the order older, middle, newest."""
+    args = []
+    keep = []
+    for off, mem in layers:
+        o, m = _csr(off, mem)
+        keep.append((o, m))
+        args += [_p(o, C.c_uint64), _p(m, C.c_uint32), len(o) - 1]
+    out = np.zeros(30, np.uint64)
+    rc = lib().hmo_strictinc30(*args, _p(out, C.c_uint64))
+    if rc != 0:
+        raise RuntimeError(f"hmo_strictinc30 failed: {rc}")
+    return out
+
+
+def vertex_triads(offsets, members) -> np.ndarray:
+    """(type1, type2, type3) vertex-triad counts."""
+    off, mem = _csr(offsets, members)
+    out = np.zeros(3, np.uint64)
+    rc = lib().hmo_vertex_triads(len(off) - 1, _p(off, C.c_uint64), _p(mem, C.c_uint32), _p(out, C.c_uint64))
+    if rc != 0:
+        raise RuntimeError(f"hmo_vertex_triads failed: {rc}")
     return out
 
 

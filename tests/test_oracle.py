@@ -10,6 +10,7 @@ from oracle import oracle
 from tests.helpers import csr, digest, load_golden, random_graph, static_case, temporal_case
 
 REF_DBLP = Path("/root/reference/MoCHy-master/dblp_graph.txt")
+ROOT = Path(__file__).resolve().parents[1]
 
 
 @pytest.mark.parametrize("name", sorted(load_golden("static")))
@@ -87,3 +88,39 @@ def test_class_rules_agree_with_oracle():
     # 30 static classes and 96 temporal motifs are each hit by some pattern
     assert {engine.classify_static(p) for p in range(128)} - {-1} == set(range(30))
     assert {engine.classify_temporal(p) for p in range(128)} - {-1} == set(range(96))
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_vertex_triads_match_reference_programs(seed, tmp_path):
+    """The restated type1/2/3 counts equal the reference's own counters
+    (temporalDynamicHMotif/src/type{1,2,3}.cpp, built by build_ref.sh)."""
+    import subprocess
+
+    from oracle import oracle, ref_runner as rr
+
+    exe = [ROOT / "oracle" / "_ref" / f"type{t}" for t in (1, 2, 3)]
+    if not all(e.exists() for e in exe):
+        pytest.skip("reference type counters not built (reference tree absent)")
+    rng = np.random.default_rng(seed)
+    off, mem = random_graph(rng, 150, 50, 10)
+    g = tmp_path / "g.txt"
+    rr.write_mochy(g, off, mem)
+    ref = [int(subprocess.run([str(e), str(g)], capture_output=True, text=True, check=True).stdout.split()[-1])
+           for e in exe]
+    assert oracle.vertex_triads(off, mem).tolist() == ref
+
+
+def test_strictinc_hand_case():
+    """One closed triple across the layers (older {0,1}, middle {1,2},
+    newest {0,2}): pairwise overlaps 1, no shared node; ids in order."""
+    from oracle import oracle
+
+    L0 = (np.array([0, 2], np.uint64), np.array([0, 1], np.uint32))
+    L1 = (np.array([0, 1, 3], np.uint64), np.array([9, 1, 2], np.uint32))
+    L2 = (np.array([0, 1, 2, 4], np.uint64), np.array([8, 7, 0, 2], np.uint32))
+    c = oracle.strictinc30([L0, L1, L2])
+    assert c.sum() == 1
+    assert c[oracle.lib().hmo_static_class(2, 2, 2, 1, 1, 1, 0)] == 1
+    # the same triple with the newest one earlier than the middle one: none
+    L2b = (np.array([0, 2, 3, 4], np.uint64), np.array([0, 2, 8, 7], np.uint32))
+    assert oracle.strictinc30([L0, L1, L2b]).sum() == 0
