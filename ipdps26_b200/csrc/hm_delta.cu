@@ -30,8 +30,13 @@ namespace {
 constexpr unsigned kWarp = 32;
 constexpr unsigned kBlock = 256;
 constexpr unsigned kWarps = kBlock / kWarp;
-constexpr unsigned kSlots = 16384;        // shared table of one marked row
+constexpr unsigned kSlots = 16384;        // shared table of one marked row (the longest rows): 208 KB
+constexpr unsigned kBigThreads = 512;     // its block: 16 warps, one block per SM
 constexpr unsigned kRowMax = kSlots / 2;  // longer rows use a global table
+constexpr unsigned kMidSlots = 4096;      // rows up to kMidRow: 4096-slot tables, 4 blocks per SM
+constexpr unsigned kMidRow = kMidSlots / 2;
+constexpr unsigned kWarpRow = 128;        // rows up to kWarpRow: one warp each, 256-slot tables
+constexpr unsigned kWarpSlots = 256;
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr unsigned kUnroll = 4;
 
@@ -165,7 +170,7 @@ struct TouchArgs {
   const uint64_t* goff;     // per item: offset of its global table (rows longer than kRowMax)
   const uint32_t* gslots;   // per item: slots of that table, 0 for a shared-memory row
   const uint32_t* brange;   // per item: [brange[2i], brange[2i+1]) of row(m) to take b from
-  const unsigned long long* gtab;
+  const uint4* gtab;        // global tables: {key, overlap, mask low, mask high}
   const uint32_t* gos;      // per slot: its graph (null: one output row)
   const uint32_t* rog;      // per graph: output row
   bool by_id;               // walk the id-ordered suffix of row(b) instead of N+(b)
@@ -215,44 +220,225 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t cm, ui
 
 __device__ __forceinline__ uint32_t hmix(uint32_t key) { return key * 2654435761u; }
 
-// Global-memory tables of the marked rows too long for shared memory: entry
-// (neighbour << 32) | index in the row, all ones when empty.
+// Global-memory tables of the marked rows too long for shared memory: one
+// 16-byte entry per key {key, overlap, mask low, mask high}, key all ones
+// when empty, so a probe answers with one load.
 __global__ void k_build_ghash(const uint32_t* ids, uint32_t n, const uint64_t* goff, const uint32_t* gslots,
                               const uint32_t* brange, const uint64_t* off, const uint32_t* len, const uint32_t* nbr,
-                              unsigned long long* tab) {
+                              const uint8_t* ovl, const uint64_t* mask, uint4* tab) {
   for (uint64_t i = global_warp(); i < n; i += n_warps()) {
     const uint32_t slots = gslots[i];
     if (!slots || brange[2 * i] != 0) continue;  // one build per row: its first slice
     const uint32_t m = ids[i];
-    unsigned long long* t = tab + goff[i];
+    uint4* t = tab + goff[i];
     const uint64_t mo = off[m];
     for (uint32_t k = lane_id(); k < len[m]; k += kWarp) {
       const uint32_t key = nbr[mo + k];
-      const unsigned long long e = ((unsigned long long)key << 32) | k;
       uint32_t h = hmix(key) & (slots - 1);
-      while (atomicCAS(&t[h], ~0ull, e) != ~0ull) h = (h + 1) & (slots - 1);
+      while (atomicCAS(&t[h].x, kEmpty, key) != kEmpty) h = (h + 1) & (slots - 1);
+      const uint64_t mk = mask[mo + k];
+      t[h].y = ovl[mo + k];
+      t[h].z = (uint32_t)mk;
+      t[h].w = (uint32_t)(mk >> 32);
     }
   }
 }
 
-// One block per marked m, heaviest rows first: row(m) in a bucketized
-// shared-memory table (4 keys per 16-byte bucket, with the row index of each
-// key) or, for rows longer than kRowMax, in a global table; warps take b in
-// row(m), lanes walk N+(b), the neighbours of b ranked above b by (degree,
-// id), with four probes in flight. A
-// triangle {m, b, c} is counted at its smallest marked id. g comes from the
-// position masks of m (|m| <= 64) or of b (|b| <= 64), else from a merge.
-// Star triangles (all overlaps 1, one shared node) are counted per size
-// category in registers.
-__global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
-  extern __shared__ uint32_t smem32[];
-  uint32_t* keys = smem32;                                         // kSlots
-  uint16_t* sidx = reinterpret_cast<uint16_t*>(keys + kSlots);     // kSlots
-  __shared__ unsigned long long wcnt[kWarps][36];
+// The table of one marked row: bucketized shared keys (4 per 16-byte bucket)
+// with each key's index in the row, or a global table for the longest rows.
+struct MarkTable {
+  const uint32_t* keys;
+  const uint8_t* sovl;    // overlap with m of each key
+  const uint64_t* smask;  // m's shared positions of each key
+  uint32_t shift, bmask;
+  uint32_t gslots;  // > 0: global table gt of gslots entries
+  const uint4* gt;
+};
+
+__device__ __forceinline__ void fill_mark_table(const TouchArgs& A, uint64_t mo, uint32_t md, uint32_t* keys,
+                                                uint8_t* sovl, uint64_t* smask, uint32_t shift, uint32_t bmask,
+                                                unsigned first, unsigned stride) {
+  for (uint32_t i = first; i < md; i += stride) {
+    const uint32_t key = A.nbr[mo + i];
+    uint32_t bk = hmix(key) >> shift, h = 0;
+    for (bool done = false; !done; bk = (bk + 1) & bmask)
+      for (uint32_t t = 0; t < 4; ++t)
+        if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
+          h = 4 * bk + t;
+          done = true;
+          break;
+        }
+    sovl[h] = A.ovl[mo + i];
+    smask[h] = A.mask[mo + i];
+  }
+}
+
+// One whole warp: the bi-th neighbour b of the marked m. Lanes walk the
+// neighbours c of b ranked above it, N+(b) by (degree, id) or the part of b's
+// id-sorted row after b, so each pair {b, c} of m's neighbours is met once,
+// from its lower-ranked end, with four probes in flight. A triangle {m, b, c}
+// is counted at its smallest marked id. g comes from the position masks of m
+// (|m| <= 64) or of b (|b| <= 64), else from a merge. Star triangles (all
+// overlaps 1, one shared node) are counted per size category in registers.
+__device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m, uint64_t mo, uint32_t sm,
+                                                 uint32_t cat_m, uint32_t bi, const MarkTable& T,
+                                                 unsigned long long* wc) {
+  const unsigned lane = lane_id();
+  const uint32_t b = A.nbr[mo + bi];
+  if (A.mark[b] && b < m) return;  // counted at b
+  const uint32_t cmb = A.ovl[mo + bi];
+  const uint32_t sb = A.esize[b];
+  uint64_t bo;
+  uint32_t bl;
+  if (A.by_id) {
+    const uint32_t split = warp_bound<true>(A.nbr + A.off[b], A.len[b], b);
+    bo = A.off[b] + split;
+    bl = A.len[b] - split;
+  } else {
+    bo = A.poff[b];
+    bl = A.plen[b];
+  }
+  const uint32_t* cnbr = A.by_id ? A.nbr : A.pnbr;
+  const uint64_t* cmask = A.by_id ? A.mask : A.pmask;
+  // masks: relative to m when |m| <= 64, else relative to b when |b| <= 64
+  const bool piv_m = sm <= 64, piv_b = !piv_m && sb <= 64;
+  uint64_t pmb = piv_m ? A.mask[mo + bi] : 0;
+  if (piv_b) {  // b's entry for m, from b's full row
+    const uint64_t fo = A.off[b];
+    pmb = A.mask[fo + warp_bound<false>(A.nbr + fo, A.len[b], m)];
+  }
+  const bool star_ok = cmb == 1 && (piv_m || piv_b);
+  uint32_t star0 = 0, star1 = 0, star2 = 0;
+  for (uint32_t j0 = 0; j0 < bl; j0 += kWarp * kUnroll) {
+    uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      const uint32_t j = j0 + u * kWarp + lane;
+      cv[u] = kEmpty;
+      ov[u] = 0;
+      if (j < bl) {
+        cv[u] = __ldg(cnbr + bo + j);
+        ov[u] = A.by_id ? ((uint32_t)__ldg(A.esize + cv[u]) << 8) | __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
+      }
+    }
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      const uint32_t c = cv[u];
+      if (c == kEmpty) continue;
+      uint32_t cmc = 0;  // overlap of c with m (0: not a neighbour of m)
+      uint64_t mmc = 0;  // m's shared positions with c
+      if (!T.gslots) {
+        uint32_t bk = hmix(c) >> T.shift;
+        int t;
+        for (;;) {
+          const uint4 q = reinterpret_cast<const uint4*>(T.keys)[bk];
+          t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
+          if (t >= 0 || q.w == kEmpty) break;
+          bk = (bk + 1) & T.bmask;
+        }
+        if (t >= 0) {
+          cmc = T.sovl[4 * bk + t];
+          mmc = T.smask[4 * bk + t];
+        }
+      } else {
+        uint32_t h = hmix(c) & (T.gslots - 1);
+        for (;;) {
+          const uint4 e = T.gt[h];
+          if (e.x == kEmpty) break;
+          if (e.x == c) {
+            cmc = e.y;
+            mmc = ((uint64_t)e.w << 32) | e.z;
+            break;
+          }
+          h = (h + 1) & (T.gslots - 1);
+        }
+      }
+      if (!cmc) continue;
+      if (A.mark[c] && c < m) continue;  // counted at c
+      const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
+      uint32_t g;
+      if (piv_m || piv_b) {
+        const uint64_t pmc = piv_m ? mmc : cmask[bo + j0 + u * kWarp + lane];
+        if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
+          const uint32_t cc = size_cat(sc);
+          star0 += cc == 0;
+          star1 += cc == 1;
+          star2 += cc == 2;
+          continue;
+        }
+        g = (uint32_t)__popcll(pmb & pmc);
+      } else {
+        g = triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
+      }
+      const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
+      if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
+      const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
+      const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
+      const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
+      const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
+      const unsigned peers = __match_any_sync(__activemask(), key);
+      if (lane == (unsigned)(__ffs(peers) - 1)) {
+        const unsigned long long cnt = (unsigned long long)__popc(peers);
+        atomicAdd(&wc[k], cnt);
+        atomicAdd(&wc[30 + om], cnt);
+        atomicAdd(&wc[30 + ob], cnt);
+        atomicAdd(&wc[30 + oc], cnt);
+      }
+    }
+  }
+  if (star_ok) {
+    for (int d = 16; d; d >>= 1) {
+      star0 += __shfl_xor_sync(0xffffffffu, star0, d);
+      star1 += __shfl_xor_sync(0xffffffffu, star1, d);
+      star2 += __shfl_xor_sync(0xffffffffu, star2, d);
+    }
+    if (lane == 0) {
+      const uint32_t cat_b = size_cat(sb);
+      if (star0) add_star(wc, cat_m, cat_b, 0, star0);
+      if (star1) add_star(wc, cat_m, cat_b, 1, star1);
+      if (star2) add_star(wc, cat_m, cat_b, 2, star2);
+    }
+  }
+}
+
+constexpr uint32_t kNoRow = 0xffffffffu;
+
+__device__ __forceinline__ void flush_touch(unsigned long long* wc, unsigned long long* out) {
+  for (unsigned k = lane_id(); k < 36; k += kWarp)
+    if (wc[k]) {
+      atomicAdd(&out[k], wc[k]);
+      wc[k] = 0;
+    }
+  __syncwarp();
+}
+
+// Output row of marked m (per-request rows of a pooled store).
+__device__ __forceinline__ uint32_t row_of(const TouchArgs& A, uint32_t m) {
+  return A.gos ? A.rog[A.gos[m]] : 0u;
+}
+
+// Shared-memory bytes of a table of `slots` entries: masks, keys, overlaps.
+constexpr size_t touch_smem(unsigned slots) {
+  return (sizeof(uint64_t) + sizeof(uint32_t) + sizeof(uint8_t)) * slots;
+}
+
+// One block per marked m, heaviest rows first: row(m) in a shared table of
+// up to kTab slots (load <= 1/2) with each key's overlap and mask or, for
+// rows longer than kRowMax, in a global table, split into slices of
+// neighbours (items [0, n_long)); warps take b in row(m).
+template <unsigned kTab, unsigned kThreads, unsigned kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_touch_closed(TouchArgs A) {
+  constexpr unsigned kW = kThreads / kWarp;
+  extern __shared__ uint64_t smem64[];
+  uint64_t* smask = smem64;                                          // kTab
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kTab);        // kTab
+  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kTab);           // kTab
+  __shared__ unsigned long long wcnt[kW][36];
   __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
   for (unsigned k = lane; k < 36; k += kWarp) wc[k] = 0;
+  uint32_t cur_row = kNoRow;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1u);
     __syncthreads();
@@ -260,192 +446,116 @@ __global__ void __launch_bounds__(kBlock, 2) k_touch_closed(TouchArgs A) {
     if (item >= A.n) break;
     const bool long_row = item < A.n_long;
     const uint32_t m = long_row ? A.ids[item] : A.short_ids[item - A.n_long];
+    const uint32_t row = row_of(A, m);
+    if (row != cur_row) {
+      if (cur_row != kNoRow) flush_touch(wc, A.out + (size_t)cur_row * kRowStride);
+      cur_row = row;
+    }
     const uint64_t mo = A.off[m];
     const uint32_t md = A.len[m];
     const uint32_t sm = A.esize[m];
-    const uint32_t gslots = long_row ? A.gslots[item] : 0u;
-    const unsigned long long* gt = A.gtab + (long_row ? A.goff[item] : 0ull);
-    uint32_t shift = 32, bmask = 0;
-    if (!gslots) {
+    MarkTable T{keys, sovl, smask, 32, 0, long_row ? A.gslots[item] : 0u, A.gtab + (long_row ? A.goff[item] : 0ull)};
+    if (!T.gslots) {
       uint32_t slots = 64;
-      while (slots < 2 * md && slots < kSlots) slots <<= 1;
+      while (slots < 2 * md && slots < kTab) slots <<= 1;
       const uint32_t buckets = slots / 4;
-      shift = 32 - (31 - __clz(buckets));
-      bmask = buckets - 1;
+      T.shift = 32 - (31 - __clz(buckets));
+      T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      for (uint32_t i = threadIdx.x; i < md; i += blockDim.x) {
-        const uint32_t key = A.nbr[mo + i];
-        uint32_t bk = hmix(key) >> shift, h = 0;
-        for (bool done = false; !done; bk = (bk + 1) & bmask)
-          for (uint32_t t = 0; t < 4; ++t)
-            if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
-              h = 4 * bk + t;
-              done = true;
-              break;
-            }
-        sidx[h] = (uint16_t)i;
-      }
+      fill_mark_table(A, mo, md, keys, sovl, smask, T.shift, T.bmask, threadIdx.x, blockDim.x);
     }
     __syncthreads();
     const uint32_t cat_m = size_cat(sm);
     const uint32_t b_begin = long_row ? A.brange[2 * item] : 0u;
     const uint32_t b_end = long_row ? A.brange[2 * item + 1] : md;
-    for (uint32_t bi = b_begin + w; bi < b_end; bi += kWarps) {
-      const uint32_t b = A.nbr[mo + bi];
-      if (A.mark[b] && b < m) continue;  // counted at b
-      const uint32_t cmb = A.ovl[mo + bi];
-      const uint32_t sb = A.esize[b];
-      // c runs over the neighbours of b ranked above it: N+(b) by (degree,
-      // id), or the part of b's id-sorted row after b. Each pair {b, c} of
-      // m's neighbours is met once, from its lower-ranked end.
-      uint64_t bo;
-      uint32_t bl;
-      if (A.by_id) {
-        const uint32_t split = warp_bound<true>(A.nbr + A.off[b], A.len[b], b);
-        bo = A.off[b] + split;
-        bl = A.len[b] - split;
-      } else {
-        bo = A.poff[b];
-        bl = A.plen[b];
-      }
-      const uint32_t* cnbr = A.by_id ? A.nbr : A.pnbr;
-      const uint64_t* cmask = A.by_id ? A.mask : A.pmask;
-      // masks: relative to m when |m| <= 64, else relative to b when |b| <= 64
-      const bool piv_m = sm <= 64, piv_b = !piv_m && sb <= 64;
-      uint64_t pmb = piv_m ? A.mask[mo + bi] : 0;
-      const uint32_t lo = 0;
-      if (piv_b) {  // b's entry for m, from b's full row
-        const uint64_t fo = A.off[b];
-        pmb = A.mask[fo + warp_bound<false>(A.nbr + fo, A.len[b], m)];
-      }
-      const bool star_ok = cmb == 1 && (piv_m || piv_b);
-      uint32_t star0 = 0, star1 = 0, star2 = 0;
-      for (uint32_t j0 = lo; j0 < bl; j0 += kWarp * kUnroll) {
-        uint32_t cv[kUnroll], ov[kUnroll];
-#pragma unroll
-        for (unsigned u = 0; u < kUnroll; ++u) {
-          const uint32_t j = j0 + u * kWarp + lane;
-          cv[u] = kEmpty;
-          ov[u] = 0;
-          if (j < bl) {
-            cv[u] = __ldg(cnbr + bo + j);
-            ov[u] = A.by_id ? ((uint32_t)__ldg(A.esize + cv[u]) << 8) | __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
-          }
-        }
-#pragma unroll
-        for (unsigned u = 0; u < kUnroll; ++u) {
-          const uint32_t c = cv[u];
-          if (c == kEmpty) continue;
-          int idx = -1;
-          if (!gslots) {
-            uint32_t bk = hmix(c) >> shift;
-            int t;
-            for (;;) {
-              const uint4 q = reinterpret_cast<const uint4*>(keys)[bk];
-              t = q.x == c ? 0 : q.y == c ? 1 : q.z == c ? 2 : q.w == c ? 3 : -1;
-              if (t >= 0 || q.w == kEmpty) break;
-              bk = (bk + 1) & bmask;
-            }
-            if (t >= 0) idx = sidx[4 * bk + t];
-          } else {
-            uint32_t h = hmix(c) & (gslots - 1);
-            for (;;) {
-              const unsigned long long e = gt[h];
-              if (e == ~0ull) break;
-              if ((uint32_t)(e >> 32) == c) {
-                idx = (int)(uint32_t)e;
-                break;
-              }
-              h = (h + 1) & (gslots - 1);
-            }
-          }
-          if (idx < 0) continue;
-          if (A.mark[c] && c < m) continue;  // counted at c
-          const uint32_t cmc = A.ovl[mo + idx];
-          const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
-          uint32_t g;
-          if (piv_m || piv_b) {
-            const uint64_t pmc = piv_m ? A.mask[mo + idx] : cmask[bo + j0 + u * kWarp + lane];
-            if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
-              const uint32_t cc = size_cat(sc);
-              star0 += cc == 0;
-              star1 += cc == 1;
-              star2 += cc == 2;
-              continue;
-            }
-            g = (uint32_t)__popcll(pmb & pmc);
-          } else {
-            g = triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
-          }
-          const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
-          if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-          const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
-          const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
-          const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
-          const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
-          const unsigned peers = __match_any_sync(__activemask(), key);
-          if (lane == (unsigned)(__ffs(peers) - 1)) {
-            const unsigned long long cnt = (unsigned long long)__popc(peers);
-            atomicAdd(&wc[k], cnt);
-            atomicAdd(&wc[30 + om], cnt);
-            atomicAdd(&wc[30 + ob], cnt);
-            atomicAdd(&wc[30 + oc], cnt);
-          }
-        }
-      }
-      if (star_ok) {
-        for (int d = 16; d; d >>= 1) {
-          star0 += __shfl_xor_sync(0xffffffffu, star0, d);
-          star1 += __shfl_xor_sync(0xffffffffu, star1, d);
-          star2 += __shfl_xor_sync(0xffffffffu, star2, d);
-        }
-        if (lane == 0) {
-          const uint32_t cat_b = size_cat(sb);
-          if (star0) add_star(wc, cat_m, cat_b, 0, star0);
-          if (star1) add_star(wc, cat_m, cat_b, 1, star1);
-          if (star2) add_star(wc, cat_m, cat_b, 2, star2);
-        }
-      }
-      __syncwarp();
-    }
-    if (A.gos) {  // per-request rows: flush this item's counts to its graph's row
-      unsigned long long* o = A.out + (size_t)A.rog[A.gos[m]] * kRowStride;
-      for (unsigned k = lane; k < 36; k += kWarp)
-        if (wc[k]) {
-          atomicAdd(&o[k], wc[k]);
-          wc[k] = 0;
-        }
+    for (uint32_t bi = b_begin + w; bi < b_end; bi += kW) {
+      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc);
       __syncwarp();
     }
     __syncthreads();
   }
   __syncwarp();
-  for (unsigned k = lane; k < 36; k += kWarp)
-    if (wc[k]) atomicAdd(&A.out[k], wc[k]);
+  flush_touch(wc, A.out + (cur_row == kNoRow ? 0 : (size_t)cur_row * kRowStride));
 }
 
-// Sort key of a marked row: [long row] [output row of its graph when gos is
-// set, 31 bits] [row length, 32 bits]. Descending order puts rows in global
-// tables first, then keeps each graph's rows together (heaviest first), so
-// that the blocks running at one time share one graph's rows in L2.
+// One warp per marked m with a short row (<= kWarpRow): a 256-slot table of
+// its own, no block-wide barriers.
+__global__ void __launch_bounds__(kBlock, 4) k_touch_warp(TouchArgs A) {
+  __shared__ __align__(16) uint32_t keys_all[kWarps][kWarpSlots];
+  __shared__ uint64_t mask_all[kWarps][kWarpSlots];
+  __shared__ uint8_t ovl_all[kWarps][kWarpSlots];
+  __shared__ unsigned long long wcnt[kWarps][36];
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  uint32_t* keys = keys_all[w];
+  uint64_t* smask = mask_all[w];
+  uint8_t* sovl = ovl_all[w];
+  unsigned long long* wc = wcnt[w];
+  for (unsigned k = lane; k < 36; k += kWarp) wc[k] = 0;
+  __syncwarp();
+  uint32_t cur_row = kNoRow;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(A.queue, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= A.n) break;
+    const uint32_t m = A.short_ids[it];
+    const uint32_t row = row_of(A, m);
+    if (row != cur_row) {
+      if (cur_row != kNoRow) flush_touch(wc, A.out + (size_t)cur_row * kRowStride);
+      cur_row = row;
+    }
+    const uint64_t mo = A.off[m];
+    const uint32_t md = A.len[m];  // <= kWarpRow by the split
+    const uint32_t sm = A.esize[m];
+    uint32_t slots = 64;
+    while (slots < 2 * md && slots < kWarpSlots) slots <<= 1;
+    const uint32_t buckets = slots / 4;
+    MarkTable T{keys, sovl, smask, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, 0u, A.gtab};
+    for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
+    __syncwarp();
+    fill_mark_table(A, mo, md, keys, sovl, smask, T.shift, T.bmask, lane, kWarp);
+    __syncwarp();
+    const uint32_t cat_m = size_cat(sm);
+    for (uint32_t bi = 0; bi < md; ++bi) {
+      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc);
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  flush_touch(wc, A.out + (cur_row == kNoRow ? 0 : (size_t)cur_row * kRowStride));
+}
+
+// Sort key of a marked row: [long row: global table] [length class, 2 bits:
+// 2 = longer than kMidRow, 1 = longer than kWarpRow] [output row of its graph
+// when gos is set, 29 bits] [row length, 32 bits]. Descending order gives the
+// three launches' lists (long and large rows, medium rows, short rows), each
+// keeping one graph's rows together and heaviest first, so that the blocks
+// running at one time share one graph's rows in L2.
 __global__ void k_touch_keys(const uint32_t* ids, uint32_t n, const uint32_t* len, const uint32_t* gos,
                              const uint32_t* rog, uint64_t* key) {
   for (uint64_t i = gtid(); i < n; i += gstride()) {
     const uint32_t m = ids[i], l = len[m];
     uint64_t k = l;
-    if (gos) k |= (uint64_t)min(rog[gos[m]], 0x7fffffffu) << 32;
+    if (gos) k |= (uint64_t)min(rog[gos[m]], 0x1fffffffu) << 32;
+    k |= (uint64_t)(l > kMidRow ? 2u : l > kWarpRow ? 1u : 0u) << 61;
     if (l > kRowMax) k |= 1ull << 63;
     key[i] = k;
   }
 }
 
-__global__ void k_count_long(const uint64_t* key, uint32_t n, unsigned int* out) {
-  for (uint64_t i = gtid(); i < n; i += gstride())
-    if (key[i] >> 63) atomicAdd(out, 1u);
+// counts[0] long rows, [1] class-2 rows (long ones included), [2] class-1 rows
+__global__ void k_count_classes(const uint64_t* key, uint32_t n, unsigned int* counts) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const uint64_t k = key[i];
+    if (k >> 63) atomicAdd(&counts[0], 1u);
+    const uint32_t cls = (uint32_t)(k >> 61) & 3u;
+    if (cls == 2) atomicAdd(&counts[1], 1u);
+    if (cls == 1) atomicAdd(&counts[2], 1u);
+  }
 }
 
-constexpr size_t touch_smem() { return (sizeof(uint32_t) + sizeof(uint16_t)) * kSlots; }
+
 
 }  // namespace
 
@@ -457,7 +567,7 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   if (!n) return HM_OK;
   const uint32_t E = g->n_slots;
   const bool by_id = g->touch_by_id;
-  const size_t n_cnt = (size_t)R * kRowStride + 2;  // + queue, + long-row count
+  const size_t n_cnt = (size_t)R * kRowStride + 5;  // + three queues, + class counts (u32 pairs)
   DArr<uint8_t> mark;
   DArr<uint32_t> flag, centres;
   DArr<uint64_t> pos;
@@ -466,8 +576,8 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   HM_TRY(flag.alloc(ctx, E));
   HM_TRY(pos.alloc(ctx, (size_t)E + 1));
   HM_TRY(cnt.alloc(ctx, n_cnt));
-  unsigned int* queue = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride);
-  unsigned int* n_long_d = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride + 1);
+  unsigned int* queues = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride);  // 3 used
+  unsigned int* classes_d = reinterpret_cast<unsigned int*>(cnt.p + (size_t)R * kRowStride + 2);  // 3 used
   HM_CUDA(cudaMemsetAsync(mark.p, 0, E, st));
   HM_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(uint32_t) * E, st));
   HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * n_cnt, st));
@@ -495,13 +605,14 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
     HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, keys.p, skeys.p, d_ids, sids.p, (int64_t)n, 0, 64,
                                                       st));
   }
-  k_count_long<<<grid_for(n, kBlock), kBlock, 0, st>>>(skeys.p, n, n_long_d);
+  k_count_classes<<<grid_for(n, kBlock), kBlock, 0, st>>>(skeys.p, n, classes_d);
   HM_LAUNCH_CHECK();
   uint64_t nc = 0;
-  unsigned int n_long = 0;
+  unsigned int hcls[3] = {0, 0, 0};
   HM_CUDA(cudaMemcpyAsync(&nc, pos.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaMemcpyAsync(&n_long, n_long_d, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaMemcpyAsync(hcls, classes_d, sizeof(hcls), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
+  const uint32_t n_long = hcls[0], n_large = hcls[1], n_mid = hcls[2];
   HM_TRY(centres.alloc(ctx, nc));
   k_list_flagged<<<grid_for(E, kBlock), kBlock, 0, st>>>(flag.p, pos.p, E, centres.p);
   HM_LAUNCH_CHECK();
@@ -513,7 +624,10 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   HM_LAUNCH_CHECK();
   static bool attr = false;
   if (!attr) {
-    HM_CUDA(cudaFuncSetAttribute(k_touch_closed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)touch_smem()));
+    HM_CUDA(cudaFuncSetAttribute(k_touch_closed<kSlots, kBigThreads, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)touch_smem(kSlots)));
+    HM_CUDA(cudaFuncSetAttribute(k_touch_closed<kMidSlots, kBlock, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)touch_smem(kMidSlots)));
     attr = true;
   }
   // long rows: split into slices of kSlice neighbours b, one item each, all
@@ -543,10 +657,10 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
     }
   }
   const uint32_t n_items_long = (uint32_t)oid.size();
-  const uint32_t n_items = n_items_long + (n - n_long);
+  const uint32_t n_items = n_items_long + (n_large - n_long);  // the large-table launch
   DArr<uint32_t> d_oid, d_oslots, d_orange;
   DArr<uint64_t> d_ooff;
-  DArr<unsigned long long> gtab;
+  DArr<uint4> gtab;
   HM_TRY(d_oid.alloc(ctx, n_items_long));
   HM_TRY(d_oslots.alloc(ctx, n_items_long));
   HM_TRY(d_orange.alloc(ctx, 2 * (size_t)n_items_long));
@@ -558,9 +672,10 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
     HM_CUDA(cudaMemcpyAsync(d_orange.p, orange.data(), sizeof(uint32_t) * 2 * n_items_long, cudaMemcpyHostToDevice,
                             st));
     HM_CUDA(cudaMemcpyAsync(d_ooff.p, ooff.data(), sizeof(uint64_t) * n_items_long, cudaMemcpyHostToDevice, st));
-    HM_CUDA(cudaMemsetAsync(gtab.p, 0xff, sizeof(unsigned long long) * gtotal, st));
+    HM_CUDA(cudaMemsetAsync(gtab.p, 0xff, sizeof(uint4) * gtotal, st));
     k_build_ghash<<<grid_for((uint64_t)n_items_long * 32, kBlock), kBlock, 0, st>>>(
-        d_oid.p, n_items_long, d_ooff.p, d_oslots.p, d_orange.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, gtab.p);
+        d_oid.p, n_items_long, d_ooff.p, d_oslots.p, d_orange.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+        g->h2h_ovl.p, g->h2h_mask.p, gtab.p);
     HM_LAUNCH_CHECK();
     // the host copies above read pageable vectors: finish them before they go
     HM_CUDA(cudaStreamSynchronize(st));
@@ -569,18 +684,52 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   TouchArgs A{d_oid.p, n_items_long, sids.p + n_long, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
               g->h2h_ovl.p, g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p,
               g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
-              rows.gos, rows.rog, by_id, queue, cnt.p};
+              rows.gos, rows.rog, by_id, queues, cnt.p};
   if (trace) cudaStreamSynchronize(st);
   auto t_cl0 = std::chrono::steady_clock::now();
-  k_touch_closed<<<std::min<unsigned>((unsigned)ctx->n_sms * 2, n_items), kBlock, touch_smem(), st>>>(A);
-  HM_LAUNCH_CHECK();
+  const unsigned sms = (unsigned)ctx->n_sms;
+  cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (trace)
+    for (auto& e : tev) cudaEventCreate(&e);
+  if (trace) cudaEventRecord(tev[0], st);
+  if (n_items) {  // long rows (global tables, sliced) and rows longer than kMidRow
+    k_touch_closed<kSlots, kBigThreads, 1><<<std::min<unsigned>(sms, n_items), kBigThreads, touch_smem(kSlots), st>>>(A);
+    HM_LAUNCH_CHECK();
+  }
+  if (trace) cudaEventRecord(tev[1], st);
+  if (n_mid) {  // rows of kWarpRow + 1 .. kMidRow
+    TouchArgs B = A;
+    B.n_long = 0;
+    B.short_ids = sids.p + n_large;
+    B.n = n_mid;
+    B.queue = queues + 1;
+    k_touch_closed<kMidSlots, kBlock, 4><<<std::min<unsigned>(sms * 4, n_mid), kBlock, touch_smem(kMidSlots), st>>>(B);
+    HM_LAUNCH_CHECK();
+  }
+  if (trace) cudaEventRecord(tev[2], st);
+  const uint32_t n_short = n - n_large - n_mid;
+  if (n_short) {  // rows of at most kWarpRow, one warp each
+    TouchArgs C = A;
+    C.n_long = 0;
+    C.short_ids = sids.p + n_large + n_mid;
+    C.n = n_short;
+    C.queue = queues + 2;
+    k_touch_warp<<<std::min<unsigned>(sms * 4, (n_short + kWarps - 1) / kWarps), kBlock, 0, st>>>(C);
+    HM_LAUNCH_CHECK();
+  }
   if (trace) {
+    cudaEventRecord(tev[3], st);
     cudaStreamSynchronize(st);
     const auto t_end = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "[hm_trace touching] marked=%u centres=%llu long=%u by_id=%d open=%.1fms closed=%.1fms\n", n,
-                 (unsigned long long)nc, n_long, (int)by_id,
+    float ms[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms[k], tev[k], tev[k + 1]);
+    for (auto& e : tev) cudaEventDestroy(e);
+    std::fprintf(stderr,
+                 "[hm_trace touching] marked=%u centres=%llu long=%u large=%u mid=%u short=%u by_id=%d open=%.1fms "
+                 "closed=%.1fms (large %.1f mid %.1f short %.1f)\n",
+                 n, (unsigned long long)nc, n_long, n_large, n_mid, n - n_large - n_mid, (int)by_id,
                  std::chrono::duration<double, std::milli>(t_cl0 - t_open0).count(),
-                 std::chrono::duration<double, std::milli>(t_end - t_cl0).count());
+                 std::chrono::duration<double, std::milli>(t_end - t_cl0).count(), ms[0], ms[1], ms[2]);
   }
   std::vector<unsigned long long> h((size_t)R * kRowStride);
   HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));

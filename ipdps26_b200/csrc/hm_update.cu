@@ -812,6 +812,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
       HM_TRY(tmp.alloc(ctx, tb));
       HM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.p, skeys.p, idx.p, sidx.p, (int64_t)n_patch, 0, 64, st));
     }
+    trace.mark("patch_sort");
     // rows of deleted or rebuilt ids, and the all-ones filler keys, are skipped
     DArr<uint8_t> keep, op;
     HM_TRY(keep.alloc(ctx, n_patch));
@@ -880,6 +881,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
       HM_TRY(exclusive_scan(ctx, remf.p, remx.p, n_kept));
       HM_TRY(exclusive_scan(ctx, addf.p, addx.p, n_kept));
       (void)need;
+      trace.mark("patch_rows");
       // Patched rows go to the arena tail in chunks that fit the free space;
       // between chunks the arena is compacted in place, so a batch never
       // needs a second copy of the store.
@@ -890,7 +892,9 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
       while (r0 < n_rows) {
         uint64_t free_space = g->h2h_cap - g->h2h_tail;
         if (hno[r0 + 1] - hno[r0] > free_space || (free_space < (hno[n_rows] - hno[r0]) && free_space < g->h2h_cap / 4)) {
+          trace.mark("patch_apply");
           HM_TRY(compact_h2h(g, hno[r0 + 1] - hno[r0]));
+          trace.mark("compact");
           free_space = g->h2h_cap - g->h2h_tail;
         }
         uint64_t r1 = r0 + 1;
