@@ -395,7 +395,7 @@ def engine_arm(args, rank, world, local_rank):
                     "traffic": traffic, "peak_kind": peak_kind,
                     "algorithmic_bytes": tr["b_static"], "kernel_model_bytes": tr["kernel_bytes"],
                     "kernel_model_gbs": tr["kernel_bytes"] / t_launch / 1e9,
-                    "kernel": "k_open_pairs + k_closed (two launch shapes): one static count",
+                    "kernel": "k_open_pairs + k_closed (three launch shapes by oriented row length): one static count",
                     "closed_ms": statistics.mean(closed_ms), "open_ms": statistics.mean(open_ms)}
         e2e = None
         if not args.no_e2e:
@@ -431,7 +431,8 @@ def engine_arm(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": config_of(args, world), "gpu_launches": 3 * args.steps,
+            # per step: k_open_pairs and the three closed-phase launch shapes
+            "config": config_of(args, world), "gpu_launches": 4 * args.steps,
             "triples_per_step": triples, "closed_triangles_per_step": closed_tri,
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
