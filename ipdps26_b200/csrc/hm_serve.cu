@@ -91,6 +91,7 @@ struct hm_server {
   std::vector<GraphIds> ids;
   // per-request mode
   std::vector<hm_graph*> graphs;
+  std::vector<int> graph_broken;  // per graph: status of a failed update that may have left it half updated
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -180,6 +181,7 @@ int build_stores(hm_server* s) {
         return rc;
       }
       s->graphs.push_back(g);
+      s->graph_broken.push_back(0);
     }
   } else {
     std::vector<uint64_t> off(1, 0);
@@ -236,9 +238,17 @@ void finish(hm_server* s, Request& r, int status) {
   r.res.done_ms = now_ms(s->t0);
 }
 
-// One request on its own store (the plain per-call form).
+// One request on its own store (the plain per-call form). An update that
+// fails for another reason than its own arguments (which are checked before
+// the store changes) may have left the graph half updated: the graph then
+// answers every later request with that status.
 void serve_one(hm_server* s, Request& r) {
   hm_graph* g = s->graphs[r.graph];
+  int& broken = s->graph_broken[r.graph];
+  if (broken) {
+    finish(s, r, broken);
+    return;
+  }
   int rc;
   if (r.kind == HM_REQ_COUNT) {
     rc = count_static30(g, 0, 1, r.res.counts30);
@@ -249,6 +259,7 @@ void serve_one(hm_server* s, Request& r) {
     rc = apply_batch(g, r.dels.data(), (uint32_t)r.dels.size(), n_ins ? r.ins_off.data() : &zero, r.ins_mem.data(),
                      n_ins, r.assigned.data(), r.res.delta30);
     r.res.n_assigned = n_ins;
+    if (rc < 0 && rc != HM_ERR_INVALID && rc != HM_ERR_NOT_LIVE && rc != HM_ERR_LIMIT) broken = rc;
   }
   finish(s, r, rc < 0 ? rc : HM_OK);
 }

@@ -204,3 +204,42 @@ def test_id_orientation_deltas_match_recount(ctx):
             _, d = g.apply_batch(dels, ins.offsets, ins.members)
             total += d
             assert g.count_static30().astype(np.int64).tolist() == total.tolist()
+
+
+@pytest.mark.parametrize("mode", ["batched", "per_request"])
+def test_failed_round_is_reported_and_later_requests_fail_cleanly(ctx, mode):
+    """Device allocation failure injected on the host in the middle of
+    serving: the failing request reports HM_ERR_NOMEM, requests that depend
+    on the damaged store report it too, none hangs, and the other graphs of
+    the per-request form keep serving."""
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HM_ERR_NOMEM, lib
+
+    ps, hs = _graphs(small=True)
+    m = engine.SERVE_BATCHED if mode == "batched" else engine.SERVE_PER_REQUEST
+    with engine.Server(ctx, m) as s:
+        for h in hs:
+            s.add_graph(h.offsets, h.members, h.n_nodes)
+        s.start()
+        ok, _ = s.wait(s.submit_update(0, [0], np.array([0, 2], np.uint64), np.array([1, 2], np.uint32)))
+        assert ok.status == 0
+        lib.hm_debug_fail_allocations_after(3)
+        try:
+            t1 = s.submit_update(1, [0, 1], np.array([0, 3], np.uint64), np.array([1, 2, 3], np.uint32))
+            s.drain()
+        finally:
+            lib.hm_debug_fail_allocations_after(-1)
+        r1, _ = s.wait(t1)
+        assert r1.status == HM_ERR_NOMEM
+        t2 = s.submit_update(1, [], np.array([0, 2], np.uint64), np.array([4, 5], np.uint32))
+        t3 = s.submit_count(2)
+        s.drain()
+        r2, _ = s.wait(t2)
+        r3, _ = s.wait(t3)
+        assert r2.status == HM_ERR_NOMEM  # the damaged store refuses further work
+        if mode == "batched":
+            assert r3.status == HM_ERR_NOMEM  # one pooled store for all graphs
+        else:
+            assert r3.status == 0  # graph 2 has its own store
+            with engine.Graph.from_hypergraph(ctx, hs[2]) as g:
+                assert list(r3.counts30) == g.count_static30().tolist()
