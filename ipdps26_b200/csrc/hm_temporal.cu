@@ -244,12 +244,14 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
   __shared__ uint32_t s_item, s_nla;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   for (unsigned k = threadIdx.x; k < 96; k += blockDim.x) cnt96[k] = 0;
+  // the table is cleared once here; after each event only the slots it used
+  // are reset (all of them after an overflow)
+  for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
   for (;;) {
     if (threadIdx.x == 0) {
       s_item = atomicAdd(A.queue, 1u);
       s_nla = 0;
     }
-    for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
     __syncthreads();
     const uint32_t p = s_item;
     if (p >= A.n) break;
@@ -316,6 +318,8 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
     const uint32_t nla = s_nla;
     if (nla > kMaxNbrs) {
       if (threadIdx.x == 0) atomicExch(A.overflow, 1);
+      for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
+      __syncthreads();
       continue;  // block-uniform; the whole count is reported as failed
     }
     const uint32_t* ao = A.opos + A.ooff[sa];
@@ -439,6 +443,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
     // 4. motif 96: two earlier occurrences of a
     if (threadIdx.x == 0 && ta_n >= 2) atomicAdd(&cnt96[95], (unsigned long long)ta_n * (ta_n - 1) / 2);
     __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nla; i += blockDim.x) keys[la[i]] = kEmpty;  // reset the used slots
   }
   __syncthreads();
   for (unsigned k = threadIdx.x; k < 96; k += blockDim.x)
