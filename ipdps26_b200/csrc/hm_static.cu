@@ -236,14 +236,51 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
 // exactly. Star triangles (all three overlaps 1, the same shared node) are
 // only counted per size category in registers; the others are classified and
 // their four counter updates aggregated across the lanes that share them.
+// Classifies the first n records of a warp's queue of closed triangles that
+// are not stars, one per lane, and adds their counts. A record packs |b|,
+// |c|, C_ab, C_bc, C_ac and g (8 bits each); sa is the centre's size.
+__device__ __forceinline__ void classify_queue(const uint64_t* q, uint32_t n, uint32_t sa, unsigned long long* wc) {
+  const unsigned lane = lane_id();
+  if (lane < n) {
+    const uint64_t r = q[lane];
+    const uint32_t sb = r & 0xffu, sc = (r >> 8) & 0xffu, cab = (r >> 16) & 0xffu, cbc = (r >> 24) & 0xffu,
+                   cac = (r >> 32) & 0xffu, g = (r >> 40) & 0xffu;
+    const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
+    if (k >= 0) {  // always, for a closed triangle; keeps the index in range
+      const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
+      const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
+      const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
+      const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
+      const unsigned peers = __match_any_sync(__activemask(), key);
+      if (lane == (unsigned)(__ffs(peers) - 1)) {
+        const unsigned long long cnt = (unsigned long long)__popc(peers);
+        atomicAdd(&wc[k], cnt);
+        atomicAdd(&wc[30 + oa], cnt);
+        atomicAdd(&wc[30 + ob], cnt);
+        atomicAdd(&wc[30 + oc], cnt);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Sizes and overlaps are at most 255, so a record fits 48 bits.
+__device__ __forceinline__ uint64_t pack_triangle(uint32_t sb, uint32_t sc, uint32_t cab, uint32_t cbc, uint32_t cac,
+                                                  uint32_t g) {
+  return (uint64_t)sb | ((uint64_t)sc << 8) | ((uint64_t)cab << 16) | ((uint64_t)cbc << 24) |
+         ((uint64_t)cac << 32) | ((uint64_t)g << 40);
+}
+
 // kTriads: instead of classes, wc[0] collects sum x * y * z over the
 // triangles, x, y, z the pairwise overlaps minus the triple overlap (all > 0;
 // star triangles give 0), the reference's type-3 vertex triads.
 template <bool kTriads>
+// Closed triangles that are not stars go to the warp's queue q (qn records,
+// warp-uniform); every 32 of them are classified together, at full width.
 __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t a, uint32_t sa, uint64_t ao,
                                                   uint32_t ad, uint32_t bi, const CentreTable& T,
                                                   unsigned long long* wc, uint32_t cat_a, bool exact_masks,
-                                                  bool flags) {
+                                                  bool flags, uint64_t* q, uint32_t& qn) {
   const unsigned lane = lane_id();
   const uint32_t b = A.pnbr[ao + bi];
   const uint32_t osb = A.pos[ao + bi];
@@ -270,7 +307,10 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
       const uint32_t c = cv[u];
-      if (c == kEmpty) continue;
+      bool push = false;
+      uint64_t rec = 0;
+      do {
+      if (c == kEmpty) break;
       uint32_t cac = 0;
       uint64_t mac = 0;
       if (T.in_smem) {
@@ -313,7 +353,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
           }
         }
       }
-      if (!cac) continue;
+      if (!cac) break;
       const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
       uint32_t g;
       if (exact_masks) {
@@ -324,7 +364,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
             star1 += cc == 1;
             star2 += cc == 2;
           }
-          continue;
+          break;
         }
         g = __popcll(mab & mac);
       } else {
@@ -332,22 +372,22 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
       }
       if (kTriads) {
         if (cab > g && cbc > g && cac > g) triads += (unsigned long long)(cab - g) * (cbc - g) * (cac - g);
-        continue;
+        break;
       }
-      const int k = static_class((int)sa, (int)sb, (int)sc, (int)cab, (int)cbc, (int)cac, (int)g);
-      if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-      // open-pair classes phase 1 gave {b,c} at a, {a,c} at b, {a,b} at c
-      const uint32_t oa = (cab + cac < sa) + 2 * ((cab < sb) + (cac < sc));
-      const uint32_t ob = (cab + cbc < sb) + 2 * ((cab < sa) + (cbc < sc));
-      const uint32_t oc = (cac + cbc < sc) + 2 * ((cac < sa) + (cbc < sb));
-      const uint32_t key = (uint32_t)k | (oa << 5) | (ob << 8) | (oc << 11);
-      const unsigned peers = __match_any_sync(__activemask(), key);
-      if (lane == (unsigned)(__ffs(peers) - 1)) {
-        const unsigned long long n = (unsigned long long)__popc(peers);
-        atomicAdd(&wc[k], n);
-        atomicAdd(&wc[30 + oa], n);
-        atomicAdd(&wc[30 + ob], n);
-        atomicAdd(&wc[30 + oc], n);
+      push = true;
+      rec = pack_triangle(sb, sc, cab, cbc, cac, g);
+      } while (false);
+      if (!kTriads) {  // warp-converged: queue this slice's classified triangles
+        const unsigned bal = __ballot_sync(0xffffffffu, push);
+        if (push) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+        qn += (uint32_t)__popc(bal);
+        if (qn >= kWarp) {
+          __syncwarp();
+          classify_queue(q, kWarp, sa, wc);
+          if (lane < qn - kWarp) q[lane] = q[kWarp + lane];
+          __syncwarp();
+          qn -= kWarp;
+        }
       }
     }
   }
@@ -395,9 +435,12 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kHashSlotsMax); // kHashSlotsMax
   uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kHashSlotsMax);    // kHashSlotsMax
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
+  __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];  // per warp: triangles waiting to be classified
   __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
+  uint64_t* q = wqueue[w];
+  uint32_t qn = 0;
   for (unsigned k = lane; k < kNumCounters; k += kWarp) wc[k] = 0;
   uint32_t cur_row = kNoRow;  // per-request rows: the row wc is collecting for
 
@@ -433,8 +476,12 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
     for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
-      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
+      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
+    }
+    if (qn) {  // the centre's last triangles (classes depend on |a|)
+      classify_queue(q, qn, sa, wc);
+      qn = 0;
     }
     __syncthreads();
   }
@@ -451,11 +498,14 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
   __shared__ uint64_t mask_all[kClosedWarps][kWarpSlots];
   __shared__ uint8_t ovl_all[kClosedWarps][kWarpSlots];
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
+  __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint32_t* keys = keys_all[w];
   uint64_t* smask = mask_all[w];
   uint8_t* sovl = ovl_all[w];
   unsigned long long* wc = wcnt[w];
+  uint64_t* q = wqueue[w];
+  uint32_t qn = 0;
   for (unsigned k = lane; k < kNumCounters; k += kWarp) wc[k] = 0;
   __syncwarp();
   uint32_t cur_row = kNoRow;
@@ -488,8 +538,12 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
     for (uint32_t bi = 0; bi < ad; ++bi) {
-      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags);
+      closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
+    }
+    if (qn) {
+      classify_queue(q, qn, sa, wc);
+      qn = 0;
     }
   }
   __syncwarp();
