@@ -203,17 +203,19 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
 // bucket), each key's overlap with the centre and shared-position mask (or
 // its row index, for the diagnostic pass). Rows too long for it are searched
 // in global memory instead.
+// One value per key: the shared-position mask when the centre has at most 64
+// members (its overlap is then the mask's popcount), else the overlap; the
+// row index in the diagnostic pass.
 struct CentreTable {
   const uint32_t* keys;
-  const uint8_t* sovl;
-  const uint64_t* smask;
+  const uint64_t* sval;
   uint32_t shift, bmask;
   bool in_smem;
 };
 
 // Fills the table with N+(a), threads t = first, first + stride, ...
-__device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys, uint8_t* sovl,
-                                           uint64_t* smask, uint32_t shift, uint32_t bmask, bool flags,
+__device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys,
+                                           uint64_t* sval, uint32_t shift, uint32_t bmask, bool flags, bool exact,
                                            unsigned first, unsigned stride) {
   for (uint32_t i = first; i < ad; i += stride) {
     const uint32_t key = A.pnbr[ao + i];
@@ -225,8 +227,7 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
           done = true;
           break;
         }
-    smask[h] = flags ? (uint64_t)i : A.pmask[ao + i];  // diagnostics keep the row index
-    sovl[h] = (uint8_t)(A.pos[ao + i] & 0xffu);
+    sval[h] = flags ? (uint64_t)i : exact ? A.pmask[ao + i] : (uint64_t)(A.pos[ao + i] & 0xffu);
   }
 }
 
@@ -323,15 +324,19 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
           bk = (bk + 1) & T.bmask;
         }
         if (t >= 0) {
-          const uint32_t h = 4 * bk + (uint32_t)t;
-          cac = T.sovl[h];
-          mac = T.smask[h];
+          const uint64_t v = T.sval[4 * bk + (uint32_t)t];
           if (flags) {
             const uint32_t j = j0 + u * kWarp + lane;
-            A.edge_flags[ao + mac] = 1;
+            A.edge_flags[ao + v] = 1;
             A.edge_flags[ao + bi] = 1;
             A.edge_flags[bo + j] = 1;
-            mac = A.pmask[ao + mac];
+            cac = A.pos[ao + v] & 0xffu;
+            mac = A.pmask[ao + v];
+          } else if (exact_masks) {
+            mac = v;
+            cac = (uint32_t)__popcll(v);
+          } else {
+            cac = (uint32_t)v;
           }
         }
       } else {
@@ -377,7 +382,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
       push = true;
       rec = pack_triangle(sb, sc, cab, cbc, cac, g);
       } while (false);
-      if (!kTriads) {  // warp-converged: queue this slice's classified triangles
+      if (!kTriads) {  // warp-converged: queue this slice's triangles (64 places)
         const unsigned bal = __ballot_sync(0xffffffffu, push);
         if (push) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
         qn += (uint32_t)__popc(bal);
@@ -431,9 +436,8 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
   constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
   extern __shared__ uint64_t smem64[];
-  uint64_t* smask = smem64;                                            // kHashSlotsMax
-  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kHashSlotsMax); // kHashSlotsMax
-  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kHashSlotsMax);    // kHashSlotsMax
+  uint64_t* sval = smem64;                                             // kHashSlotsMax
+  uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kHashSlotsMax);  // kHashSlotsMax
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];  // per warp: triangles waiting to be classified
   __shared__ uint32_t s_item;
@@ -461,7 +465,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t ad = A.plen[a];
     const uint32_t sa = A.esize[a];
     const bool flags = A.edge_flags != nullptr;
-    CentreTable T{keys, sovl, smask, 32, 0, ad <= kHashRowMax};
+    CentreTable T{keys, sval, 32, 0, ad <= kHashRowMax};
     if (T.in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
@@ -470,7 +474,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_table(A, ao, ad, keys, sovl, smask, T.shift, T.bmask, flags, threadIdx.x, blockDim.x);
+      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x);
     }
     __syncthreads();
     const uint32_t cat_a = size_cat(sa);
@@ -495,14 +499,12 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
 template <bool kTriads = false>
 __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
   __shared__ __align__(16) uint32_t keys_all[kClosedWarps][kWarpSlots];
-  __shared__ uint64_t mask_all[kClosedWarps][kWarpSlots];
-  __shared__ uint8_t ovl_all[kClosedWarps][kWarpSlots];
+  __shared__ uint64_t val_all[kClosedWarps][kWarpSlots];
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint32_t* keys = keys_all[w];
-  uint64_t* smask = mask_all[w];
-  uint8_t* sovl = ovl_all[w];
+  uint64_t* sval = val_all[w];
   unsigned long long* wc = wcnt[w];
   uint64_t* q = wqueue[w];
   uint32_t qn = 0;
@@ -530,10 +532,10 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     uint32_t slots = 64;
     while (slots < 2 * ad && slots < kWarpSlots) slots <<= 1;
     const uint32_t buckets = slots / 4;
-    CentreTable T{keys, sovl, smask, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true};
+    CentreTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true};
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
     __syncwarp();
-    fill_table(A, ao, ad, keys, sovl, smask, T.shift, T.bmask, flags, lane, kWarp);
+    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp);
     __syncwarp();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
@@ -586,7 +588,7 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
 
 }  // namespace
 
-constexpr size_t closed_smem_bytes(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t) + 1) * slots; }
+constexpr size_t closed_smem_bytes(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t)) * slots; }
 constexpr unsigned kBigSlots = 8192, kSmallSlots = 4096;
 
 // Centres that own at least one oriented wedge, heaviest first.
