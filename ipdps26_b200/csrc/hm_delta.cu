@@ -23,6 +23,7 @@
 #include "hm_classes.h"
 #include "hm_device.h"
 #include "hm_pairs.cuh"
+#include "hm_triangles.cuh"
 
 namespace hm {
 namespace {
@@ -30,7 +31,7 @@ namespace {
 constexpr unsigned kWarp = 32;
 constexpr unsigned kBlock = 256;
 constexpr unsigned kWarps = kBlock / kWarp;
-constexpr unsigned kSlots = 16384;        // shared table of one marked row (the longest rows): 208 KB
+constexpr unsigned kSlots = 16384;        // shared table of one marked row (the longest rows): 192 KB
 constexpr unsigned kBigThreads = 512;     // its block: 16 warps, one block per SM
 constexpr unsigned kRowMax = kSlots / 2;  // longer rows use a global table
 constexpr unsigned kMidSlots = 4096;      // rows up to kMidRow: 4096-slot tables, 4 blocks per SM
@@ -246,17 +247,18 @@ __global__ void k_build_ghash(const uint32_t* ids, uint32_t n, const uint64_t* g
 
 // The table of one marked row: bucketized shared keys (4 per 16-byte bucket)
 // with each key's index in the row, or a global table for the longest rows.
+// One value per key: m's shared-position mask with it when |m| <= 64 (the
+// overlap is its popcount), else the overlap.
 struct MarkTable {
   const uint32_t* keys;
-  const uint8_t* sovl;    // overlap with m of each key
-  const uint64_t* smask;  // m's shared positions of each key
+  const uint64_t* sval;
   uint32_t shift, bmask;
   uint32_t gslots;  // > 0: global table gt of gslots entries
   const uint4* gt;
 };
 
-__device__ __forceinline__ void fill_mark_table(const TouchArgs& A, uint64_t mo, uint32_t md, uint32_t* keys,
-                                                uint8_t* sovl, uint64_t* smask, uint32_t shift, uint32_t bmask,
+__device__ __forceinline__ void fill_mark_table(const TouchArgs& A, uint64_t mo, uint32_t md, bool exact,
+                                                uint32_t* keys, uint64_t* sval, uint32_t shift, uint32_t bmask,
                                                 unsigned first, unsigned stride) {
   for (uint32_t i = first; i < md; i += stride) {
     const uint32_t key = A.nbr[mo + i];
@@ -268,8 +270,7 @@ __device__ __forceinline__ void fill_mark_table(const TouchArgs& A, uint64_t mo,
           done = true;
           break;
         }
-    sovl[h] = A.ovl[mo + i];
-    smask[h] = A.mask[mo + i];
+    sval[h] = exact ? A.mask[mo + i] : (uint64_t)A.ovl[mo + i];
   }
 }
 
@@ -280,12 +281,14 @@ __device__ __forceinline__ void fill_mark_table(const TouchArgs& A, uint64_t mo,
 // is counted at its smallest marked id. g comes from the position masks of m
 // (|m| <= 64) or of b (|b| <= 64), else from a merge. Star triangles (all
 // overlaps 1, one shared node) are counted per size category in registers.
+// Triangles that are not stars go to the warp's queue q (qn records,
+// warp-uniform), classified 32 at a time.
 __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m, uint64_t mo, uint32_t sm,
                                                  uint32_t cat_m, uint32_t bi, const MarkTable& T,
-                                                 unsigned long long* wc) {
+                                                 unsigned long long* wc, uint64_t* q, uint32_t& qn) {
   const unsigned lane = lane_id();
   const uint32_t b = A.nbr[mo + bi];
-  if (A.mark[b] && b < m) return;  // counted at b
+  if (A.mark[b] && b < m) return;  // counted at b (warp-uniform)
   const uint32_t cmb = A.ovl[mo + bi];
   const uint32_t sb = A.esize[b];
   uint64_t bo;
@@ -324,7 +327,10 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
       const uint32_t c = cv[u];
-      if (c == kEmpty) continue;
+      bool push = false;
+      uint64_t rec = 0;
+      do {
+      if (c == kEmpty) break;
       uint32_t cmc = 0;  // overlap of c with m (0: not a neighbour of m)
       uint64_t mmc = 0;  // m's shared positions with c
       if (!T.gslots) {
@@ -337,8 +343,13 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
           bk = (bk + 1) & T.bmask;
         }
         if (t >= 0) {
-          cmc = T.sovl[4 * bk + t];
-          mmc = T.smask[4 * bk + t];
+          const uint64_t v = T.sval[4 * bk + t];
+          if (piv_m) {  // |m| <= 64: the mask is exact
+            mmc = v;
+            cmc = (uint32_t)__popcll(v);
+          } else {
+            cmc = (uint32_t)v;
+          }
         }
       } else {
         uint32_t h = hmix(c) & (T.gslots - 1);
@@ -353,8 +364,8 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
           h = (h + 1) & (T.gslots - 1);
         }
       }
-      if (!cmc) continue;
-      if (A.mark[c] && c < m) continue;  // counted at c
+      if (!cmc) break;
+      if (A.mark[c] && c < m) break;  // counted at c
       const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
       uint32_t g;
       if (piv_m || piv_b) {
@@ -364,25 +375,25 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
           star0 += cc == 0;
           star1 += cc == 1;
           star2 += cc == 2;
-          continue;
+          break;
         }
         g = (uint32_t)__popcll(pmb & pmc);
       } else {
         g = triple_overlap3(A.hoff, A.hmem, A.esize, m, b, c);
       }
-      const int k = static_class((int)sm, (int)sb, (int)sc, (int)cmb, (int)cbc, (int)cmc, (int)g);
-      if (k < 0) continue;  // cannot happen for a closed triangle; keeps the index in range
-      const uint32_t om = (cmb + cmc < sm) + 2 * ((cmb < sb) + (cmc < sc));
-      const uint32_t ob = (cmb + cbc < sb) + 2 * ((cmb < sm) + (cbc < sc));
-      const uint32_t oc = (cmc + cbc < sc) + 2 * ((cmc < sm) + (cbc < sb));
-      const uint32_t key = (uint32_t)k | (om << 5) | (ob << 8) | (oc << 11);
-      const unsigned peers = __match_any_sync(__activemask(), key);
-      if (lane == (unsigned)(__ffs(peers) - 1)) {
-        const unsigned long long cnt = (unsigned long long)__popc(peers);
-        atomicAdd(&wc[k], cnt);
-        atomicAdd(&wc[30 + om], cnt);
-        atomicAdd(&wc[30 + ob], cnt);
-        atomicAdd(&wc[30 + oc], cnt);
+      push = true;
+      rec = pack_triangle(sb, sc, cmb, cbc, cmc, g);
+      } while (false);
+      // warp-converged: queue this slice's triangles (64 places)
+      const unsigned bal = __ballot_sync(0xffffffffu, push);
+      if (push) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+      qn += (uint32_t)__popc(bal);
+      if (qn >= kWarp) {
+        __syncwarp();
+        classify_queue(q, kWarp, sm, wc);
+        if (lane < qn - kWarp) q[lane] = q[kWarp + lane];
+        __syncwarp();
+        qn -= kWarp;
       }
     }
   }
@@ -418,9 +429,7 @@ __device__ __forceinline__ uint32_t row_of(const TouchArgs& A, uint32_t m) {
 }
 
 // Shared-memory bytes of a table of `slots` entries: masks, keys, overlaps.
-constexpr size_t touch_smem(unsigned slots) {
-  return (sizeof(uint64_t) + sizeof(uint32_t) + sizeof(uint8_t)) * slots;
-}
+constexpr size_t touch_smem(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t)) * slots; }
 
 // One block per marked m, heaviest rows first: row(m) in a shared table of
 // up to kTab slots (load <= 1/2) with each key's overlap and mask or, for
@@ -430,13 +439,15 @@ template <unsigned kTab, unsigned kThreads, unsigned kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_touch_closed(TouchArgs A) {
   constexpr unsigned kW = kThreads / kWarp;
   extern __shared__ uint64_t smem64[];
-  uint64_t* smask = smem64;                                          // kTab
-  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kTab);        // kTab
-  uint8_t* sovl = reinterpret_cast<uint8_t*>(keys + kTab);           // kTab
+  uint64_t* sval = smem64;                                           // kTab
+  uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kTab);         // kTab
   __shared__ unsigned long long wcnt[kW][36];
+  __shared__ uint64_t wqueue[kW][2 * kWarp];  // per warp: triangles waiting to be classified
   __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
+  uint64_t* q = wqueue[w];
+  uint32_t qn = 0;
   for (unsigned k = lane; k < 36; k += kWarp) wc[k] = 0;
   uint32_t cur_row = kNoRow;
   for (;;) {
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_touch_closed(TouchArgs
     const uint64_t mo = A.off[m];
     const uint32_t md = A.len[m];
     const uint32_t sm = A.esize[m];
-    MarkTable T{keys, sovl, smask, 32, 0, long_row ? A.gslots[item] : 0u, A.gtab + (long_row ? A.goff[item] : 0ull)};
+    MarkTable T{keys, sval, 32, 0, long_row ? A.gslots[item] : 0u, A.gtab + (long_row ? A.goff[item] : 0ull)};
     if (!T.gslots) {
       uint32_t slots = 64;
       while (slots < 2 * md && slots < kTab) slots <<= 1;
@@ -463,15 +474,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_touch_closed(TouchArgs
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_mark_table(A, mo, md, keys, sovl, smask, T.shift, T.bmask, threadIdx.x, blockDim.x);
+      fill_mark_table(A, mo, md, sm <= 64, keys, sval, T.shift, T.bmask, threadIdx.x, blockDim.x);
     }
     __syncthreads();
     const uint32_t cat_m = size_cat(sm);
     const uint32_t b_begin = long_row ? A.brange[2 * item] : 0u;
     const uint32_t b_end = long_row ? A.brange[2 * item + 1] : md;
     for (uint32_t bi = b_begin + w; bi < b_end; bi += kW) {
-      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc);
+      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc, q, qn);
       __syncwarp();
+    }
+    if (qn) {  // this item's last triangles (classes depend on |m|)
+      classify_queue(q, qn, sm, wc);
+      qn = 0;
     }
     __syncthreads();
   }
@@ -483,14 +498,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_touch_closed(TouchArgs
 // its own, no block-wide barriers.
 __global__ void __launch_bounds__(kBlock, 4) k_touch_warp(TouchArgs A) {
   __shared__ __align__(16) uint32_t keys_all[kWarps][kWarpSlots];
-  __shared__ uint64_t mask_all[kWarps][kWarpSlots];
-  __shared__ uint8_t ovl_all[kWarps][kWarpSlots];
+  __shared__ uint64_t val_all[kWarps][kWarpSlots];
   __shared__ unsigned long long wcnt[kWarps][36];
+  __shared__ uint64_t wqueue[kWarps][2 * kWarp];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint32_t* keys = keys_all[w];
-  uint64_t* smask = mask_all[w];
-  uint8_t* sovl = ovl_all[w];
+  uint64_t* sval = val_all[w];
   unsigned long long* wc = wcnt[w];
+  uint64_t* q = wqueue[w];
+  uint32_t qn = 0;
   for (unsigned k = lane; k < 36; k += kWarp) wc[k] = 0;
   __syncwarp();
   uint32_t cur_row = kNoRow;
@@ -511,15 +527,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_touch_warp(TouchArgs A) {
     uint32_t slots = 64;
     while (slots < 2 * md && slots < kWarpSlots) slots <<= 1;
     const uint32_t buckets = slots / 4;
-    MarkTable T{keys, sovl, smask, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, 0u, A.gtab};
+    MarkTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, 0u, A.gtab};
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
     __syncwarp();
-    fill_mark_table(A, mo, md, keys, sovl, smask, T.shift, T.bmask, lane, kWarp);
+    fill_mark_table(A, mo, md, sm <= 64, keys, sval, T.shift, T.bmask, lane, kWarp);
     __syncwarp();
     const uint32_t cat_m = size_cat(sm);
     for (uint32_t bi = 0; bi < md; ++bi) {
-      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc);
+      touch_pairs_of_b(A, m, mo, sm, cat_m, bi, T, wc, q, qn);
       __syncwarp();
+    }
+    if (qn) {
+      classify_queue(q, qn, sm, wc);
+      qn = 0;
     }
   }
   __syncwarp();
