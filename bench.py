@@ -393,6 +393,7 @@ def engine_arm(args, rank, world, local_rank):
                     traffic = tj.get("dram_bytes_per_step")
             roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                     "traffic": traffic, "peak_kind": peak_kind,
+                    "traffic_gbs": traffic / t_launch / 1e9 if traffic else None,
                     "algorithmic_bytes": tr["b_static"], "kernel_model_bytes": tr["kernel_bytes"],
                     "kernel_model_gbs": tr["kernel_bytes"] / t_launch / 1e9,
                     "kernel": "k_open_pairs + k_closed (three launch shapes by oriented row length): one static count",
