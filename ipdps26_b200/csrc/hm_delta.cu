@@ -432,7 +432,7 @@ __device__ __forceinline__ uint32_t row_of(const TouchArgs& A, uint32_t m) {
 constexpr size_t touch_smem(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t)) * slots; }
 
 // One block per marked m, heaviest rows first: row(m) in a shared table of
-// up to kTab slots (load <= 1/2) with each key's overlap and mask or, for
+// up to kTab slots (load <= 1/2) with one value per key (mask or overlap) or, for
 // rows longer than kRowMax, in a global table, split into slices of
 // neighbours (items [0, n_long)); warps take b in row(m).
 template <unsigned kTab, unsigned kThreads, unsigned kMinBlocks>

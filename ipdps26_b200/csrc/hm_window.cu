@@ -14,9 +14,10 @@
 // newest), reused until a layer changes. Kernel: one block per middle j. Its
 // H2H row is sorted by slot, so the older neighbours i < j are a prefix and
 // the newest neighbours k > j a suffix; the suffix goes into a shared table
-// with each entry's overlap and shared-position mask, warps take i, and lanes
-// walk the newest suffix of row(i) probing the table. g = |i & j & k| is
-// popc(mask_ji & mask_jk) for |j| <= 64, else a three-way merge.
+// (each key with its position in row(j), whose overlap and shared-position
+// mask a hit then reads), warps take i, and lanes walk the newest suffix of
+// row(i) probing the table. g = |i & j & k| is popc(mask_ji & mask_jk) for
+// |j| <= 64, else a three-way merge.
 #include <algorithm>
 #include <cstdio>
 #include <fstream>
