@@ -226,7 +226,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
                       const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks);
 int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
                 const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
-int presize_h2h(hm_graph* g);
+int presize_h2h(hm_graph* g, uint32_t factor);
 
 inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
   uint64_t b = (items + per_block - 1) / per_block;

@@ -35,6 +35,13 @@ namespace {
 
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr unsigned kBlock = 256;
+// H2H arena headroom at start, in multiples of the live entries. The pooled
+// store compacts one arena shared by every graph, so it gets more room
+// between compactions; per-graph stores keep what the first batch would
+// give them (measured on the served workload: 3x made the pool 12 % faster
+// and the per-graph stores slower).
+constexpr uint32_t kPoolHeadroom = 3;
+constexpr uint32_t kStoreHeadroom = 2;
 
 __global__ void k_set_gos(const uint32_t* slots, const uint32_t* graph, uint32_t n, uint32_t* gos) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -175,7 +182,7 @@ int build_stores(hm_server* s) {
       int rc = build_h2v(g, st.off.data(), st.mem.data(), n);
       if (rc >= 0) rc = build_v2h(g);
       if (rc >= 0) rc = build_h2h_rows(g);
-      if (rc >= 0) rc = presize_h2h(g);
+      if (rc >= 0) rc = presize_h2h(g, kStoreHeadroom);
       if (rc < 0) {
         delete g;
         return rc;
@@ -212,7 +219,7 @@ int build_stores(hm_server* s) {
     int rc = build_h2v(g, off.data(), mem.data(), n);
     if (rc >= 0) rc = build_v2h(g);
     if (rc >= 0) rc = build_h2h_rows(g);
-    if (rc >= 0) rc = presize_h2h(g);
+    if (rc >= 0) rc = presize_h2h(g, kPoolHeadroom);
     if (rc < 0) {
       delete g;
       return rc;

@@ -543,11 +543,11 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   return regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
 }
 
-// Grows the H2H arena to the size the first batch would grow it to (twice
-// the live entries), so that a store about to take a stream of batches pays
-// for the growth up front.
-int presize_h2h(hm_graph* g) {
-  const uint64_t want = 2 * g->h2h_nnz + 1024;
+// Grows the H2H arena to `factor` times the live entries (the first batch
+// would grow it to twice), so that a store about to take a stream of batches
+// pays for the growth up front.
+int presize_h2h(hm_graph* g, uint32_t factor) {
+  const uint64_t want = (uint64_t)factor * g->h2h_nnz + 1024;
   return g->h2h_cap < want ? regrow_h2h(g, want) : (int)HM_OK;
 }
 
