@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--no-traffic", action="store_true")
     ap.add_argument("--write-traffic", default=None,
                     help="compute the algorithmic bytes of this workload live and write them to this JSON file")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default closed-phase schedule")
+    ap.add_argument("--tune-stride", type=int, default=0,
+                    help="autotuner sample: every n-th centre (0: at most 65536 centres)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
@@ -334,6 +337,17 @@ def engine_arm(args, rank, world, local_rank):
     g = engine.Graph.from_hypergraph(ctx, h)
     stream = torch.cuda.ExternalStream(engine.lib.hm_ctx_stream(ctx.handle))
 
+    # the launch schedule, picked by the autotuner on rank 0 before any timing;
+    # every rank must split the work list the same way for the shards to add up
+    tune = None
+    if not args.no_tune:
+        if rank == 0:
+            tune = g.autotune(args.tune_stride).as_dict()
+        if world > 1:
+            sched = torch.tensor(list(g.schedule), dtype=torch.int64, device=f"cuda:{local_rank}")
+            dist.broadcast(sched, 0)
+            g.set_schedule(*[int(x) for x in sched.tolist()])
+
     def step():
         part = g.count_static30_shard(rank, world)
         if world > 1:
@@ -396,7 +410,8 @@ def engine_arm(args, rank, world, local_rank):
                     "traffic_gbs": traffic / t_launch / 1e9 if traffic else None,
                     "algorithmic_bytes": tr["b_static"], "kernel_model_bytes": tr["kernel_bytes"],
                     "kernel_model_gbs": tr["kernel_bytes"] / t_launch / 1e9,
-                    "kernel": "k_open_pairs + k_closed (three launch shapes by oriented row length): one static count",
+                    "kernel": "k_open_pairs + k_closed (three launch shapes split by the tuned schedule, "
+                              "replayed as two captured CUDA graphs): one static count",
                     "closed_ms": statistics.mean(closed_ms), "open_ms": statistics.mean(open_ms)}
         e2e = None
         if not args.no_e2e:
@@ -409,6 +424,7 @@ def engine_arm(args, rank, world, local_rank):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 with engine.Graph(ctx, off, mem, h.n_nodes) as g2:
+                    g2.set_schedule(*g.schedule)  # the tuned schedule of this workload
                     c26 = g2.count_static()
                 times.append(time.perf_counter() - t0)
             e2e = {"value": int(c26.sum()) / statistics.mean(times), "unit": UNIT,
@@ -421,6 +437,7 @@ def engine_arm(args, rank, world, local_rank):
         updates = None
         if args.update_batches > 0:
             updates = update_section(args, g, p, counts)
+        g_sched = g.schedule
         g.close()  # the sections below build their own stores
         temporal = None
         if not args.no_temporal:
@@ -433,7 +450,8 @@ def engine_arm(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             # per step: k_open_pairs and the three closed-phase launch shapes
-            "config": config_of(args, world), "gpu_launches": 4 * args.steps,
+            "config": {**config_of(args, world), "schedule": list(g_sched)}, "gpu_launches": 4 * args.steps,
+            "autotune": tune,
             "triples_per_step": triples, "closed_triangles_per_step": closed_tri,
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),

@@ -133,6 +133,26 @@ extern "C" int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_s
   return hm::count_static30(g, shard, n_shards, out30);
 }
 
+extern "C" int hm_graph_set_schedule(hm_graph* g, const hm_schedule* s) {
+  if (!g || !s) return hm::set_error(HM_ERR_INVALID, "hm_graph_set_schedule: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::set_schedule(g, hm::ClosedSchedule{s->warp_row, s->small_row});
+}
+
+extern "C" int hm_graph_get_schedule(const hm_graph* g, hm_schedule* s) {
+  if (!g || !s) return hm::set_error(HM_ERR_INVALID, "hm_graph_get_schedule: NULL argument");
+  s->warp_row = g->sched.warp_row;
+  s->small_row = g->sched.small_row;
+  return HM_OK;
+}
+
+extern "C" int hm_graph_autotune(hm_graph* g, uint32_t sample_stride, hm_tune_report* report) {
+  if (!g) return hm::set_error(HM_ERR_INVALID, "hm_graph_autotune: NULL graph");
+  HM_TRY(static_ok(g));
+  CtxLock lock(g->ctx);
+  return hm::autotune_closed(g, sample_stride, report);
+}
+
 extern "C" int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]) {
   if (!g || !out26) return hm::set_error(HM_ERR_INVALID, "hm_count_static: NULL argument");
   HM_TRY(static_ok(g));

@@ -88,6 +88,32 @@ struct PhaseTimes {
   uint64_t closed_triangles = 0;
 };
 
+// Which launch shape of the closed phase takes a centre, by the length d of
+// its oriented row: d <= warp_row one warp each (warp_row <= 128, the warp
+// kernel's 256-slot tables), d <= small_row blocks with 4096-slot tables,
+// longer rows blocks with 8192-slot tables. Counts never depend on it.
+struct ClosedSchedule {
+  uint32_t warp_row = 128;
+  uint32_t small_row = 2048;
+};
+
+// Launch sequences of the static count captured as CUDA graphs (open phase,
+// closed phase), replayed while the arguments they were captured with hold.
+struct CountCapture {
+  static constexpr unsigned kKey = 20;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  uint64_t key[kKey] = {};
+  bool valid = false;
+  void reset() {
+    for (auto& e : exec)
+      if (e) {
+        cudaGraphExecDestroy(e);
+        e = nullptr;
+      }
+    valid = false;
+  }
+};
+
 }  // namespace hm
 
 // The device-resident hypergraph. Three segment tables share one layout:
@@ -147,9 +173,11 @@ struct hm_graph {
   uint32_t n_work = 0;
   uint32_t n_work_big = 0;  // the first n_work_big centres have rows longer than the small-table limit
   uint32_t n_work_mid = 0;  // centres [n_work_big, n_work_mid) have rows longer than the warp-kernel limit
+  hm::ClosedSchedule sched; // the split of the work list into launch shapes
   hm::DArr<unsigned long long> counters;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool ev_ready = false;
+  hm::CountCapture capture;
 
   // temporal (optional): timestamps per slot and the time-ordered index
   hm::DArr<int64_t> ts;
@@ -169,6 +197,7 @@ struct hm_graph {
   hm::PhaseTimes times;
 
   ~hm_graph() {
+    capture.reset();
     if (ev_ready)
       for (auto& e : ev) cudaEventDestroy(e);
   }
@@ -202,6 +231,8 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
 int finish_static(hm_graph* g, uint64_t out30[30]);
 int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
 int count_vertex_triads(hm_graph* g, uint64_t out3[3]);
+int set_schedule(hm_graph* g, const ClosedSchedule& s);
+int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report* report);
 
 // Touched-triple counts (hm_delta.cu). With gos set, the triples of each
 // touched hyperedge's graph gos[slot] go to output row rog[gos[slot]]

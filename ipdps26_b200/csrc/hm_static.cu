@@ -45,12 +45,13 @@ constexpr unsigned kClosedBlock = 256;
 constexpr unsigned kClosedWarps = kClosedBlock / kWarp;
 constexpr unsigned kUnroll = 4;               // probes in flight per lane
 constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair classes
-// Two launch shapes of the closed phase: rows up to kSmallRow with a 4096-slot
-// bucketized table (4 blocks per SM, load <= 1/2), longer rows with an
-// 8192-slot table (2 per SM).
+// Block launch shapes of the closed phase: rows up to the schedule's
+// small_row with a 4096-slot bucketized table (4 blocks per SM), longer rows
+// with an 8192-slot table (2 per SM). kSmallRow is the largest small_row the
+// 4096-slot table holds in shared memory (load <= 1/2).
 constexpr unsigned kSmallRow = 2048;
-// Rows up to kWarpRow go to the warp-per-centre kernel (a 256-slot table per
-// warp, load <= 1/2).
+// Rows up to the schedule's warp_row go to the warp-per-centre kernel; its
+// 256-slot table per warp holds at most kWarpRow entries (load <= 1/2).
 constexpr unsigned kWarpRow = 128;
 constexpr unsigned kWarpSlots = 256;
 constexpr uint32_t kEmpty = 0xffffffffu;
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   flush_counts(wc, A.out + (cur_row == kNoRow ? 0 : (size_t)cur_row * kRowStride));
 }
 
-// One warp per centre, for short oriented rows (<= kWarpRow): each warp
+// One warp per centre, for short oriented rows (<= warp_row <= kWarpRow): each warp
 // holds its own table (load <= 1/2) and walks all of N+(a) itself, with no
 // block-wide barriers; warps take centres from the queue one at a time.
 template <bool kTriads = false>
@@ -493,7 +494,7 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
       }
     }
     const uint64_t ao = A.poff[a];
-    const uint32_t ad = A.plen[a];  // <= kWarpRow by the work split
+    const uint32_t ad = A.plen[a];  // <= warp_row <= kWarpRow by the work split
     const uint32_t sa = A.esize[a];
     uint32_t slots = 64;
     while (slots < 2 * ad && slots < kWarpSlots) slots <<= 1;
@@ -520,14 +521,16 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
 
 // Work estimate per centre: sum of d+(b) over b in N+(a); centres with fewer
 // than two oriented neighbours own no triangle and are dropped (key 0). Key
-// layout: bit 63 = row longer than kSmallRow (large-table launch), bit 62 =
-// row longer than kWarpRow (block launch), then the estimate; descending
+// layout: bit 63 = row longer than small_row (large-table launch), bit 62 =
+// row longer than warp_row (block launch; warp_row <= small_row, so the
+// large-table rows carry it too), then the estimate; descending
 // order gives the three launches' lists, heaviest first. With gos set
 // (per-request rows of a pooled store) bits 40..61 hold the output row of the
 // centre's graph above a 40-bit estimate, so that the blocks running at one
 // time share one graph's rows in L2.
 __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr, const uint32_t* rows,
-                              uint32_t n, const uint32_t* gos, const uint32_t* rog, uint64_t* est, uint32_t* ids) {
+                              uint32_t n, const uint32_t* gos, const uint32_t* rog, ClosedSchedule sched,
+                              uint64_t* est, uint32_t* ids) {
   for (uint64_t r = global_warp(); r < n; r += n_warps()) {
     const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint32_t d = plen[a];
@@ -543,8 +546,8 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
           key = ((uint64_t)min(rog[gos[a]], (1u << 22) - 1u) << 40) | (e < (1ull << 40) ? e : (1ull << 40) - 1);
         else
           key = e < (1ull << 62) ? e : (1ull << 62) - 1;
-        if (d > kWarpRow) key |= 1ull << 62;
-        if (d > kSmallRow) key |= 1ull << 63;
+        if (d > sched.warp_row) key |= 1ull << 62;
+        if (d > sched.small_row) key |= 1ull << 63;
       }
       est[r] = key;
       ids[r] = a;
@@ -569,7 +572,7 @@ static int closed_worklist(hm_graph* g) {
   HM_TRY(ids.alloc(ctx, E));
   HM_TRY(g->work.alloc(ctx, E));
   k_closed_work<<<grid_for((uint64_t)E * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p,
-                                                                nullptr, E, nullptr, nullptr, est.p, ids.p);
+                                                                nullptr, E, nullptr, nullptr, g->sched, est.p, ids.p);
   HM_LAUNCH_CHECK();
   size_t tb = 0;
   HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, g->work.p, (int64_t)E,
@@ -597,7 +600,7 @@ static int closed_worklist(hm_graph* g) {
     else hi = mid;
   }
   g->n_work_big = lo;
-  hi = g->n_work;  // rows longer than kWarpRow carry bit 62 (the big ones too)
+  hi = g->n_work;  // rows longer than warp_row carry bit 62 (the big ones too)
   while (lo < hi) {
     uint32_t mid = (lo + hi) / 2;
     if ((h[mid] >> 62) & 1u) lo = mid + 1;
@@ -641,7 +644,7 @@ int prepare_static(hm_graph* g) {
 }
 
 // The closed phase over a work list split at bounds[0..3]: rows longer than
-// kSmallRow (8192-slot tables, 2 blocks per SM), rows longer than kWarpRow
+// small_row (8192-slot tables, 2 blocks per SM), rows longer than warp_row
 // (4096-slot tables, 4 blocks per SM), then the short rows, one warp each.
 // queues holds three zeroed counters, one per launch.
 template <bool kTriads = false>
@@ -670,28 +673,86 @@ static int launch_closed(hm_ctx* ctx, ClosedArgs base, const uint32_t bounds[4],
   return HM_OK;
 }
 
+// Captures the launches body() makes on stream st as an executable graph.
+template <class F>
+static int capture_graph(cudaStream_t st, F&& body, cudaGraphExec_t* exec) {
+  HM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  const int s = body();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (s < 0 || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (s < 0) return s;
+    return set_error(HM_ERR_CUDA, "stream capture of the static count: %s", cudaGetErrorString(e));
+  }
+  const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    *exec = nullptr;
+    return set_error(HM_ERR_CUDA, "graph instantiation of the static count: %s", cudaGetErrorString(ei));
+  }
+  return HM_OK;
+}
+
 // Launches both phases for one shard of the centres; the counters land in
 // g->counters ([0,30) closed classes, [30,36) open-pair removals, [36,42)
 // open-pair counts, [42..44] work queues). edge_flags is for diagnostics.
+// Each phase is captured once as a CUDA graph and replayed while everything
+// its launches were captured with (store and work-list arrays, the split,
+// the shard) is unchanged; the diagnostic form launches directly.
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
-  HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 48, st));
-  HM_CUDA(cudaEventRecord(g->ev[0], st));
-  if (E) {
-    k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
-                                                                 g->h2h_ovl.p, g->esize.p, nullptr, E, shard,
-                                                                 n_shards, nullptr, nullptr, dev + 36);
-    HM_LAUNCH_CHECK();
-  }
-  HM_CUDA(cudaEventRecord(g->ev[1], st));
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  HM_TRY(launch_closed(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
-                                       g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->work.p, 0, shard, n_shards, nullptr,
-                                       dev, edge_flags, nullptr, nullptr},
-                       bounds, reinterpret_cast<unsigned int*>(dev + 42)));
+  const ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
+                        g->h2v_off.p,  g->h2v_mem.p,  g->esize.p,    g->work.p,    0,
+                        shard,         n_shards,      nullptr,       dev,          edge_flags,
+                        nullptr,       nullptr};
+  auto open_phase = [&]() -> int {
+    HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 48, st));
+    if (E) {
+      k_open_pairs<<<(unsigned)ctx->n_sms * 8, kOpenBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+                                                                   g->h2h_ovl.p, g->esize.p, nullptr, E, shard,
+                                                                   n_shards, nullptr, nullptr, dev + 36);
+      HM_LAUNCH_CHECK();
+    }
+    return HM_OK;
+  };
+  auto closed_phase = [&]() -> int {
+    return launch_closed(ctx, args, bounds, reinterpret_cast<unsigned int*>(dev + 42));
+  };
+  if (edge_flags) {
+    HM_CUDA(cudaEventRecord(g->ev[0], st));
+    HM_TRY(open_phase());
+    HM_CUDA(cudaEventRecord(g->ev[1], st));
+    HM_TRY(closed_phase());
+    HM_CUDA(cudaEventRecord(g->ev[2], st));
+    return HM_OK;
+  }
+  const uint64_t key[CountCapture::kKey] = {
+      (uint64_t)g->h2h_off.p,  (uint64_t)g->h2h_len.p,  (uint64_t)g->h2h_nbr.p,   (uint64_t)g->h2h_ovl.p,
+      (uint64_t)g->esize.p,    (uint64_t)g->plus_off.p, (uint64_t)g->plus_len.p,  (uint64_t)g->plus_nbr.p,
+      (uint64_t)g->plus_os.p,  (uint64_t)g->plus_mask.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
+      (uint64_t)g->work.p,     (uint64_t)dev,            E,                       g->n_work,
+      g->n_work_big,           g->n_work_mid,            shard,                   n_shards};
+  CountCapture& C = g->capture;
+  bool same = C.valid;
+  for (unsigned k = 0; k < CountCapture::kKey && same; ++k) same = C.key[k] == key[k];
+  if (!same) {
+    C.reset();
+    HM_TRY(capture_graph(st, open_phase, &C.exec[0]));
+    bool any_closed = false;
+    for (int part = 0; part < 3; ++part) any_closed = any_closed || bounds[part + 1] - bounds[part] > shard;
+    if (any_closed) HM_TRY(capture_graph(st, closed_phase, &C.exec[1]));
+    for (unsigned k = 0; k < CountCapture::kKey; ++k) C.key[k] = key[k];
+    C.valid = true;
+  }
+  HM_CUDA(cudaEventRecord(g->ev[0], st));
+  HM_CUDA(cudaGraphLaunch(C.exec[0], st));
+  HM_CUDA(cudaEventRecord(g->ev[1], st));
+  if (C.exec[1]) HM_CUDA(cudaGraphLaunch(C.exec[1], st));
   HM_CUDA(cudaEventRecord(g->ev[2], st));
   return HM_OK;
 }
@@ -753,7 +814,7 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * n_cnt, st));
   unsigned long long* tail = cnt.p + (size_t)R * kRowStride;
   k_closed_work<<<grid_for((uint64_t)n * 32, 256), 256, 0, st>>>(P.off.p, P.len.p, P.nbr.p, d_rows, n, rows.gos,
-                                                                rows.rog, est.p, ids.p);
+                                                                rows.rog, g->sched, est.p, ids.p);
   HM_LAUNCH_CHECK();
   {
     size_t tb = 0;
@@ -855,6 +916,122 @@ int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out3
   HM_TRY(prepare_static(g));
   HM_TRY(launch_static(g, shard, n_shards, nullptr));
   return finish_static(g, out30);
+}
+
+int set_schedule(hm_graph* g, const ClosedSchedule& s) {
+  if (s.warp_row > kWarpRow || s.small_row < s.warp_row || s.small_row > kSmallRow)
+    return set_error(HM_ERR_INVALID, "schedule {warp_row %u, small_row %u}: need warp_row <= %u and "
+                     "warp_row <= small_row <= %u", s.warp_row, s.small_row, kWarpRow, kSmallRow);
+  if (s.warp_row != g->sched.warp_row || s.small_row != g->sched.small_row) {
+    g->sched = s;
+    g->work_valid = false;  // the work list is split by the schedule
+  }
+  return HM_OK;
+}
+
+namespace {
+// Every stride-th centre of a work list, in order.
+__global__ void k_stride_sample(const uint32_t* work, uint32_t n_out, uint32_t stride, uint32_t* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = work[i * stride];
+}
+
+struct EventPair {
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  ~EventPair() {
+    for (auto x : e)
+      if (x) cudaEventDestroy(x);
+  }
+};
+
+// Candidate schedules; the first is the default. The warp kernel's limit
+// moves rows between one warp and one block per centre, the small-table
+// limit moves rows between 4-per-SM and 2-per-SM blocks.
+constexpr ClosedSchedule kTuneCandidates[] = {{128, 2048}, {96, 2048}, {64, 2048}, {32, 2048}, {0, 2048},
+                                              {128, 1024}, {64, 1024}, {128, 512}};
+constexpr unsigned kTuneCount = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
+constexpr uint32_t kTuneSampleMax = 65536;  // sampled centres with stride 0
+constexpr float kTuneMargin = 0.98f;        // another schedule must beat the default by 2 %
+static_assert(kTuneCount <= HM_TUNE_MAX_CANDIDATES, "report holds every candidate");
+}  // namespace
+
+// Times the closed phase under every candidate schedule on one strided
+// sample of the graph's centres: the sample is fixed, each candidate splits
+// it into its own launch shapes (work estimates, sort, split as for a full
+// count) and runs the three launches into scratch counters.
+int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report* report) {
+  const auto t_begin = std::chrono::steady_clock::now();
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  HM_TRY(prepare_static(g));
+  hm_tune_report R{};
+  R.n_candidates = kTuneCount;
+  for (unsigned c = 0; c < kTuneCount; ++c) {
+    R.candidates[c].warp_row = kTuneCandidates[c].warp_row;
+    R.candidates[c].small_row = kTuneCandidates[c].small_row;
+  }
+  const uint32_t n_work = g->n_work;
+  if (stride == 0) stride = std::max<uint32_t>(1, (uint32_t)(((uint64_t)n_work + kTuneSampleMax - 1) / kTuneSampleMax));
+  R.sample_stride = stride;
+  const uint32_t n = n_work ? (uint32_t)(((uint64_t)n_work + stride - 1) / stride) : 0;
+  R.sampled = n;
+  uint32_t best = 0;
+  if (n) {
+    DArr<uint32_t> sample, ids, work;
+    DArr<uint64_t> est, est_sorted;
+    DArr<unsigned long long> cnt;
+    HM_TRY(sample.alloc(ctx, n));
+    HM_TRY(ids.alloc(ctx, n));
+    HM_TRY(work.alloc(ctx, n));
+    HM_TRY(est.alloc(ctx, n));
+    HM_TRY(est_sorted.alloc(ctx, n));
+    HM_TRY(cnt.alloc(ctx, 48));
+    size_t tb = 0;
+    HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, est.p, est_sorted.p, ids.p, work.p, (int64_t)n,
+                                                      0, 64, st));
+    DArr<uint8_t> tmp;
+    HM_TRY(tmp.alloc(ctx, tb));
+    k_stride_sample<<<grid_for(n, 256), 256, 0, st>>>(g->work.p, n, stride, sample.p);
+    HM_LAUNCH_CHECK();
+    EventPair ev;
+    HM_CUDA(cudaEventCreate(&ev.e[0]));
+    HM_CUDA(cudaEventCreate(&ev.e[1]));
+    unsigned int* wc = reinterpret_cast<unsigned int*>(cnt.p + 44);  // three work counts
+    for (int rep = -1; rep < (int)kTuneCount; ++rep) {  // rep -1: untimed warm-up of the default
+      const unsigned c = rep < 0 ? 0u : (unsigned)rep;
+      HM_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * 48, st));
+      k_closed_work<<<grid_for((uint64_t)n * 32, 256), 256, 0, st>>>(g->plus_off.p, g->plus_len.p, g->plus_nbr.p,
+                                                                    sample.p, n, nullptr, nullptr,
+                                                                    kTuneCandidates[c], est.p, ids.p);
+      HM_LAUNCH_CHECK();
+      HM_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, est.p, est_sorted.p, ids.p, work.p, (int64_t)n,
+                                                        0, 64, st));
+      k_count_work<<<grid_for(n, 256), 256, 0, st>>>(est_sorted.p, n, wc);
+      HM_LAUNCH_CHECK();
+      unsigned int hw[3] = {0, 0, 0};
+      HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
+      HM_CUDA(cudaStreamSynchronize(st));
+      const uint32_t bounds[4] = {0, hw[1], hw[2], hw[0]};
+      HM_CUDA(cudaEventRecord(ev.e[0], st));
+      HM_TRY(launch_closed(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
+                                           g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, work.p, 0, 0, 1,
+                                           nullptr, cnt.p, nullptr, nullptr, nullptr},
+                           bounds, reinterpret_cast<unsigned int*>(cnt.p + 42)));
+      HM_CUDA(cudaEventRecord(ev.e[1], st));
+      HM_CUDA(cudaEventSynchronize(ev.e[1]));
+      float ms = 0;
+      HM_CUDA(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
+      if (rep >= 0) R.ms[c] = ms;
+    }
+    for (unsigned c = 1; c < kTuneCount; ++c)
+      if (R.ms[c] < kTuneMargin * R.ms[0] && R.ms[c] < R.ms[best]) best = c;
+  }
+  R.best = best;
+  HM_TRY(set_schedule(g, kTuneCandidates[best]));
+  R.tune_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+  if (report) *report = R;
+  return HM_OK;
 }
 
 }  // namespace hm

@@ -57,6 +57,42 @@ class Timings(C.Structure):
     ]
 
 
+class Schedule(C.Structure):
+    """Launch split of the closed-triangle phase (hm_schedule)."""
+
+    _fields_ = [("warp_row", C.c_uint32), ("small_row", C.c_uint32)]
+
+    def astuple(self) -> tuple[int, int]:
+        return (self.warp_row, self.small_row)
+
+
+TUNE_MAX_CANDIDATES = 16
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("n_candidates", C.c_uint32),
+        ("best", C.c_uint32),
+        ("sample_stride", C.c_uint32),
+        ("sampled", C.c_uint32),
+        ("candidates", Schedule * TUNE_MAX_CANDIDATES),
+        ("ms", C.c_float * TUNE_MAX_CANDIDATES),
+        ("tune_ms", C.c_float),
+        ("pad_", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        n = self.n_candidates
+        return {
+            "schedule": list(self.candidates[self.best].astuple()),
+            "default": list(self.candidates[0].astuple()),
+            "sample_stride": self.sample_stride,
+            "sampled_centres": self.sampled,
+            "candidates": [[*self.candidates[i].astuple(), round(float(self.ms[i]), 3)] for i in range(n)],
+            "tune_ms": round(float(self.tune_ms), 1),
+        }
+
+
 class ServeConfig(C.Structure):
     _fields_ = [
         ("mode", C.c_int32),
@@ -118,6 +154,9 @@ _lib.bind(
         "hm_count_temporal": (C.c_int, [vp, C.c_int64, u64p]),
         "hm_debug_touch_orientation": (C.c_int, [vp, C.c_int]),
         "hm_count_vertex_triads": (C.c_int, [vp, u64p]),
+        "hm_graph_set_schedule": (C.c_int, [vp, C.POINTER(Schedule)]),
+        "hm_graph_get_schedule": (C.c_int, [vp, C.POINTER(Schedule)]),
+        "hm_graph_autotune": (C.c_int, [vp, C.c_uint32, C.POINTER(TuneReport)]),
         "hm_serve_create": (C.c_int, [vp, C.POINTER(ServeConfig), C.POINTER(vp)]),
         "hm_serve_add_graph": (C.c_int, [vp, u64p, u32p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_serve_start": (C.c_int, [vp]),
@@ -283,6 +322,24 @@ class Graph:
         out = np.zeros(3, np.uint64)
         check(lib.hm_count_vertex_triads(self._h, ptr(out, C.c_uint64)), "hm_count_vertex_triads")
         return out
+
+    @property
+    def schedule(self) -> tuple[int, int]:
+        """(warp_row, small_row) of the closed-phase launch split."""
+        sc = Schedule()
+        check(lib.hm_graph_get_schedule(self._h, C.byref(sc)), "hm_graph_get_schedule")
+        return sc.astuple()
+
+    def set_schedule(self, warp_row: int, small_row: int) -> None:
+        sc = Schedule(warp_row, small_row)
+        check(lib.hm_graph_set_schedule(self._h, C.byref(sc)), "hm_graph_set_schedule")
+
+    def autotune(self, sample_stride: int = 0) -> TuneReport:
+        """Times the candidate schedules on a sample of the centres and keeps
+        the fastest (hm_graph_autotune)."""
+        r = TuneReport()
+        check(lib.hm_graph_autotune(self._h, int(sample_stride), C.byref(r)), "hm_graph_autotune")
+        return r
 
     def set_touch_orientation(self, by_id: bool) -> None:
         """Walk order of the touched-triple counts (same counts either way)."""

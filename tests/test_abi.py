@@ -99,7 +99,7 @@ def test_struct_layouts_match_ctypes(tmp_path):
     structs = {
         "hm_graph_info_t": engine.GraphInfo, "hm_traffic_t": engine.Traffic, "hm_timings_t": engine.Timings,
         "hm_serve_config": engine.ServeConfig, "hm_serve_result": engine.ServeResult,
-        "hm_serve_stats_t": engine.ServeStats,
+        "hm_serve_stats_t": engine.ServeStats, "hm_schedule": engine.Schedule, "hm_tune_report": engine.TuneReport,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hmotif.h"', "int main(void) {"]
     for cname, py in structs.items():
