@@ -266,37 +266,54 @@ typedef struct hm_traffic_t {
 } hm_traffic_t;
 int hm_graph_traffic(hm_graph* g, hm_traffic_t* t);
 
-/* ---- launch schedule of the static count, and its autotuner --------------
- * The closed-triangle phase runs three persistent launch shapes over one
- * heaviest-first list of centres, split by the length d of each centre's
- * oriented row: d <= warp_row one warp per centre (warp_row <= 128),
- * d <= small_row one 256-thread block per centre with a 4096-slot table
- * (warp_row <= small_row <= 2048), longer rows blocks with an 8192-slot
- * table. Counts never depend on the schedule; speed does. Default
- * {128, 2048}. The reference has one launch shape, a thread per hyperedge
- * (dynamicHyperGraph/src/HMotifCount.cu:97-125). */
+/* ---- launch schedules, and their autotuner --------------------------------
+ * Static count: the closed-triangle phase runs three persistent launch
+ * shapes over one heaviest-first list of centres, split by the length d of
+ * each centre's oriented row: d <= warp_row one warp per centre
+ * (warp_row <= 128), d <= small_row one 256-thread block per centre with a
+ * 4096-slot table (warp_row <= small_row <= 2048), longer rows blocks with an
+ * 8192-slot table. Touched-triple count (the delta of every update batch):
+ * the same three shapes per marked hyperedge m by the length of its row:
+ * <= touch_warp_row one warp (<= 128), <= touch_mid_row 4096-slot blocks
+ * (touch_warp_row <= touch_mid_row <= 2048), longer rows 512-thread blocks
+ * with a 16384-slot table or a global table. Counts never depend on the
+ * schedule; speed does. Default {128, 2048, 128, 2048}. The reference has
+ * one launch shape, a thread per hyperedge
+ * (dynamicHyperGraph/src/HMotifCount.cu:97-125,
+ * src/HMotifCountUpdate.cu:150-226). */
 typedef struct hm_schedule {
   uint32_t warp_row;
   uint32_t small_row;
+  uint32_t touch_warp_row;
+  uint32_t touch_mid_row;
 } hm_schedule;
 int hm_graph_set_schedule(hm_graph* g, const hm_schedule* s);
 int hm_graph_get_schedule(const hm_graph* g, hm_schedule* s);
 
 #define HM_TUNE_MAX_CANDIDATES 16
 typedef struct hm_tune_report {
+  /* static count: (warp_row, small_row) candidates, [0] the default */
   uint32_t n_candidates;
-  uint32_t best;          /* index of the schedule now in use */
-  uint32_t sample_stride; /* every sample_stride-th centre of each shape's list was timed */
+  uint32_t best;          /* index of the pair now in use */
+  uint32_t sample_stride; /* every sample_stride-th centre of the work list was timed */
   uint32_t sampled;       /* centres in the timed sample */
-  hm_schedule candidates[HM_TUNE_MAX_CANDIDATES]; /* candidates[0] is the default */
-  float ms[HM_TUNE_MAX_CANDIDATES];                /* closed-phase device time of the sample */
+  uint32_t rows[HM_TUNE_MAX_CANDIDATES][2];
+  float ms[HM_TUNE_MAX_CANDIDATES];       /* closed-phase device time of the sample */
+  /* touched-triple count: (touch_warp_row, touch_mid_row) candidates */
+  uint32_t touch_n_candidates;
+  uint32_t touch_best;
+  uint32_t touch_sampled; /* live hyperedges marked in the timed count */
+  uint32_t touch_rows[HM_TUNE_MAX_CANDIDATES][2];
+  float touch_ms[HM_TUNE_MAX_CANDIDATES]; /* wall time of the count of the sample */
   float tune_ms;          /* wall time of the whole tuning call */
-  uint32_t pad_;
 } hm_tune_report;
-/* Times the closed phase of g under each candidate schedule on the same
- * strided sample of its centres (sample_stride 0: at most 65536 sampled
- * centres, 1: all) with CUDA events, and keeps the fastest; the default
- * stays unless another is at least 2 % faster. report may be NULL. */
+/* Times each candidate schedule of the two counts with the same input for
+ * all candidates, and keeps the fastest of each; a default stays unless
+ * another is at least 2 % faster. Static count: the closed phase on a
+ * strided sample of the centres (sample_stride 0: at most 65536 centres,
+ * 1: all), CUDA-event time. Touched-triple count: the count of every n-th
+ * live hyperedge (about 4096 of them, as a deletion batch marks them).
+ * report may be NULL. */
 int hm_graph_autotune(hm_graph* g, uint32_t sample_stride, hm_tune_report* report);
 
 /* Device times of the last count / update call on this graph (CUDA events

@@ -1,5 +1,6 @@
 // C ABI entry points for graphs: build, destroy, info, query, static counts.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -136,13 +137,16 @@ extern "C" int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_s
 extern "C" int hm_graph_set_schedule(hm_graph* g, const hm_schedule* s) {
   if (!g || !s) return hm::set_error(HM_ERR_INVALID, "hm_graph_set_schedule: NULL argument");
   CtxLock lock(g->ctx);
-  return hm::set_schedule(g, hm::ClosedSchedule{s->warp_row, s->small_row});
+  return hm::set_schedule(g, hm::ClosedSchedule{s->warp_row, s->small_row},
+                          hm::TouchSchedule{s->touch_warp_row, s->touch_mid_row});
 }
 
 extern "C" int hm_graph_get_schedule(const hm_graph* g, hm_schedule* s) {
   if (!g || !s) return hm::set_error(HM_ERR_INVALID, "hm_graph_get_schedule: NULL argument");
   s->warp_row = g->sched.warp_row;
   s->small_row = g->sched.small_row;
+  s->touch_warp_row = g->tsched.warp_row;
+  s->touch_mid_row = g->tsched.mid_row;
   return HM_OK;
 }
 
@@ -150,7 +154,13 @@ extern "C" int hm_graph_autotune(hm_graph* g, uint32_t sample_stride, hm_tune_re
   if (!g) return hm::set_error(HM_ERR_INVALID, "hm_graph_autotune: NULL graph");
   HM_TRY(static_ok(g));
   CtxLock lock(g->ctx);
-  return hm::autotune_closed(g, sample_stride, report);
+  const auto t0 = std::chrono::steady_clock::now();
+  hm_tune_report R{};
+  HM_TRY(hm::autotune_closed(g, sample_stride, R));
+  HM_TRY(hm::autotune_touch(g, R));
+  R.tune_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (report) *report = R;
+  return HM_OK;
 }
 
 extern "C" int hm_count_static(hm_graph* g, uint64_t out26[HM_N_STATIC_MOTIFS]) {

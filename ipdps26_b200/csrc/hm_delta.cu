@@ -34,9 +34,9 @@ constexpr unsigned kWarps = kBlock / kWarp;
 constexpr unsigned kSlots = 16384;        // shared table of one marked row (the longest rows): 192 KB
 constexpr unsigned kBigThreads = 512;     // its block: 16 warps, one block per SM
 constexpr unsigned kRowMax = kSlots / 2;  // longer rows use a global table
-constexpr unsigned kMidSlots = 4096;      // rows up to kMidRow: 4096-slot tables, 4 blocks per SM
+constexpr unsigned kMidSlots = 4096;      // rows up to mid_row <= kMidRow: 4096-slot tables, 4 blocks per SM
 constexpr unsigned kMidRow = kMidSlots / 2;
-constexpr unsigned kWarpRow = 128;        // rows up to kWarpRow: one warp each, 256-slot tables
+constexpr unsigned kWarpRow = 128;        // rows up to warp_row <= kWarpRow: one warp each, 256-slot tables
 constexpr unsigned kWarpSlots = 256;
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr unsigned kUnroll = 4;
@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_touch_warp(TouchArgs A) {
       cur_row = row;
     }
     const uint64_t mo = A.off[m];
-    const uint32_t md = A.len[m];  // <= kWarpRow by the split
+    const uint32_t md = A.len[m];  // <= warp_row <= kWarpRow by the split
     const uint32_t sm = A.esize[m];
     uint32_t slots = 64;
     while (slots < 2 * md && slots < kWarpSlots) slots <<= 1;
@@ -547,18 +547,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_touch_warp(TouchArgs A) {
 }
 
 // Sort key of a marked row: [long row: global table] [length class, 2 bits:
-// 2 = longer than kMidRow, 1 = longer than kWarpRow] [output row of its graph
+// 2 = longer than the schedule's mid_row, 1 = longer than its warp_row; the
+// long rows are class 2 too, as mid_row <= kMidRow] [output row of its graph
 // when gos is set, 29 bits] [row length, 32 bits]. Descending order gives the
 // three launches' lists (long and large rows, medium rows, short rows), each
 // keeping one graph's rows together and heaviest first, so that the blocks
 // running at one time share one graph's rows in L2.
 __global__ void k_touch_keys(const uint32_t* ids, uint32_t n, const uint32_t* len, const uint32_t* gos,
-                             const uint32_t* rog, uint64_t* key) {
+                             const uint32_t* rog, TouchSchedule ts, uint64_t* key) {
   for (uint64_t i = gtid(); i < n; i += gstride()) {
     const uint32_t m = ids[i], l = len[m];
     uint64_t k = l;
     if (gos) k |= (uint64_t)min(rog[gos[m]], 0x1fffffffu) << 32;
-    k |= (uint64_t)(l > kMidRow ? 2u : l > kWarpRow ? 1u : 0u) << 61;
+    k |= (uint64_t)(l > ts.mid_row ? 2u : l > ts.warp_row ? 1u : 0u) << 61;
     if (l > kRowMax) k |= 1ull << 63;
     key[i] = k;
   }
@@ -614,7 +615,8 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   HM_TRY(keys.alloc(ctx, n));
   HM_TRY(skeys.alloc(ctx, n));
   HM_TRY(sids.alloc(ctx, n));
-  k_touch_keys<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, rows.gos, rows.rog, keys.p);
+  k_touch_keys<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_ids, n, g->h2h_len.p, rows.gos, rows.rog, g->tsched,
+                                                       keys.p);
   HM_LAUNCH_CHECK();
   {
     size_t tb = 0;
@@ -712,12 +714,12 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   if (trace)
     for (auto& e : tev) cudaEventCreate(&e);
   if (trace) cudaEventRecord(tev[0], st);
-  if (n_items) {  // long rows (global tables, sliced) and rows longer than kMidRow
+  if (n_items) {  // long rows (global tables, sliced) and rows longer than mid_row
     k_touch_closed<kSlots, kBigThreads, 1><<<std::min<unsigned>(sms, n_items), kBigThreads, touch_smem(kSlots), st>>>(A);
     HM_LAUNCH_CHECK();
   }
   if (trace) cudaEventRecord(tev[1], st);
-  if (n_mid) {  // rows of kWarpRow + 1 .. kMidRow
+  if (n_mid) {  // rows of warp_row + 1 .. mid_row
     TouchArgs B = A;
     B.n_long = 0;
     B.short_ids = sids.p + n_large;
@@ -728,7 +730,7 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   }
   if (trace) cudaEventRecord(tev[2], st);
   const uint32_t n_short = n - n_large - n_mid;
-  if (n_short) {  // rows of at most kWarpRow, one warp each
+  if (n_short) {  // rows of at most warp_row, one warp each
     TouchArgs C = A;
     C.n_long = 0;
     C.short_ids = sids.p + n_large + n_mid;
@@ -765,6 +767,73 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
 
 int count_touching(hm_graph* g, const uint32_t* d_ids, uint32_t n, uint64_t out30[30]) {
   return count_touching_rows(g, d_ids, n, TouchRows{}, out30);
+}
+
+namespace {
+// Candidate touched-triple schedules; the first is the default. The warp
+// limit moves rows between one warp and one block per marked hyperedge, the
+// mid limit moves rows between 4096-slot blocks (4 per SM) and the
+// 16384-slot block (1 per SM).
+constexpr TouchSchedule kTouchCandidates[] = {{128, 2048}, {64, 2048}, {32, 2048}, {0, 2048},
+                                              {128, 1024}, {64, 1024}, {128, 512}};
+constexpr unsigned kTouchCount = sizeof(kTouchCandidates) / sizeof(kTouchCandidates[0]);
+constexpr uint32_t kTouchSample = 4096;  // marked hyperedges in the timed count
+constexpr double kTouchMargin = 0.98;    // another schedule must beat the default by 2 %
+static_assert(kTouchCount <= HM_TUNE_MAX_CANDIDATES, "report holds every candidate");
+}  // namespace
+
+// Times the touched-triple count of one set of live hyperedges (every n-th
+// live id, about kTouchSample of them, as a batch's uniform deletions mark
+// them) under each candidate schedule, by the wall time of the whole count.
+int autotune_touch(hm_graph* g, hm_tune_report& R) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  R.touch_n_candidates = kTouchCount;
+  for (unsigned c = 0; c < kTouchCount; ++c) {
+    R.touch_rows[c][0] = kTouchCandidates[c].warp_row;
+    R.touch_rows[c][1] = kTouchCandidates[c].mid_row;
+  }
+  const uint32_t words = (g->n_slots + 31) / 32;
+  std::vector<uint32_t> bits(words);
+  if (words)
+    HM_CUDA(cudaMemcpyAsync(bits.data(), g->live_bits.p, sizeof(uint32_t) * words, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  const uint32_t stride = std::max<uint32_t>(1, g->n_live / kTouchSample);
+  std::vector<uint32_t> sample;
+  uint32_t k = 0;
+  for (uint32_t id = 0; id < g->n_slots; ++id)
+    if ((bits[id >> 5] >> (id & 31)) & 1u) {
+      if (k % stride == 0) sample.push_back(id);
+      ++k;
+    }
+  const uint32_t n = (uint32_t)sample.size();
+  R.touch_sampled = n;
+  uint32_t best = 0;
+  if (n) {
+    DArr<uint32_t> d;
+    HM_TRY(d.alloc(ctx, n));
+    HM_CUDA(cudaMemcpyAsync(d.p, sample.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    const TouchSchedule keep = g->tsched;
+    uint64_t out[30];
+    for (int rep = -1; rep < (int)kTouchCount; ++rep) {  // rep -1: untimed warm-up of the default
+      const unsigned c = rep < 0 ? 0u : (unsigned)rep;
+      g->tsched = kTouchCandidates[c];
+      const auto t0 = std::chrono::steady_clock::now();
+      const int s = count_touching_rows(g, d.p, n, TouchRows{}, out);  // ends with the counts on the host
+      if (s < 0) {
+        g->tsched = keep;
+        return s;
+      }
+      if (rep >= 0)
+        R.touch_ms[c] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    g->tsched = keep;
+    for (unsigned c = 1; c < kTouchCount; ++c)
+      if (R.touch_ms[c] < kTouchMargin * R.touch_ms[0] && R.touch_ms[c] < R.touch_ms[best]) best = c;
+  }
+  R.touch_best = best;
+  return set_schedule(g, g->sched, kTouchCandidates[best]);
 }
 
 }  // namespace hm

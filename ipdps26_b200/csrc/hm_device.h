@@ -97,6 +97,14 @@ struct ClosedSchedule {
   uint32_t small_row = 2048;
 };
 
+// The same for the touched-triple count, by the length of a marked
+// hyperedge's row: <= warp_row one warp each (<= 128), <= mid_row blocks with
+// 4096-slot tables (<= 2048), longer rows 16384-slot or global tables.
+struct TouchSchedule {
+  uint32_t warp_row = 128;
+  uint32_t mid_row = 2048;
+};
+
 // Launch sequences of the static count captured as CUDA graphs (open phase,
 // closed phase), replayed while the arguments they were captured with hold.
 struct CountCapture {
@@ -174,6 +182,7 @@ struct hm_graph {
   uint32_t n_work_big = 0;  // the first n_work_big centres have rows longer than the small-table limit
   uint32_t n_work_mid = 0;  // centres [n_work_big, n_work_mid) have rows longer than the warp-kernel limit
   hm::ClosedSchedule sched; // the split of the work list into launch shapes
+  hm::TouchSchedule tsched; // the split of marked rows in touched-triple counts
   hm::DArr<unsigned long long> counters;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   bool ev_ready = false;
@@ -231,8 +240,11 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
 int finish_static(hm_graph* g, uint64_t out30[30]);
 int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
 int count_vertex_triads(hm_graph* g, uint64_t out3[3]);
-int set_schedule(hm_graph* g, const ClosedSchedule& s);
-int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report* report);
+int set_schedule(hm_graph* g, const ClosedSchedule& s, const TouchSchedule& t);
+// The autotuner's two parts: static count (hm_static.cu), touched-triple
+// count (hm_delta.cu); each fills its half of the report.
+int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report& report);
+int autotune_touch(hm_graph* g, hm_tune_report& report);
 
 // Touched-triple counts (hm_delta.cu). With gos set, the triples of each
 // touched hyperedge's graph gos[slot] go to output row rog[gos[slot]]

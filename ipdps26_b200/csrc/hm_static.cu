@@ -918,14 +918,20 @@ int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out3
   return finish_static(g, out30);
 }
 
-int set_schedule(hm_graph* g, const ClosedSchedule& s) {
+// The touched-triple launch shapes hold the same row lengths as the static
+// ones: one warp up to 128 entries, 4096-slot tables up to 2048.
+int set_schedule(hm_graph* g, const ClosedSchedule& s, const TouchSchedule& t) {
   if (s.warp_row > kWarpRow || s.small_row < s.warp_row || s.small_row > kSmallRow)
     return set_error(HM_ERR_INVALID, "schedule {warp_row %u, small_row %u}: need warp_row <= %u and "
                      "warp_row <= small_row <= %u", s.warp_row, s.small_row, kWarpRow, kSmallRow);
+  if (t.warp_row > kWarpRow || t.mid_row < t.warp_row || t.mid_row > kSmallRow)
+    return set_error(HM_ERR_INVALID, "schedule {touch_warp_row %u, touch_mid_row %u}: need touch_warp_row <= %u "
+                     "and touch_warp_row <= touch_mid_row <= %u", t.warp_row, t.mid_row, kWarpRow, kSmallRow);
   if (s.warp_row != g->sched.warp_row || s.small_row != g->sched.small_row) {
     g->sched = s;
     g->work_valid = false;  // the work list is split by the schedule
   }
+  g->tsched = t;
   return HM_OK;
 }
 
@@ -960,16 +966,14 @@ static_assert(kTuneCount <= HM_TUNE_MAX_CANDIDATES, "report holds every candidat
 // sample of the graph's centres: the sample is fixed, each candidate splits
 // it into its own launch shapes (work estimates, sort, split as for a full
 // count) and runs the three launches into scratch counters.
-int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report* report) {
-  const auto t_begin = std::chrono::steady_clock::now();
+int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report& R) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   HM_TRY(prepare_static(g));
-  hm_tune_report R{};
   R.n_candidates = kTuneCount;
   for (unsigned c = 0; c < kTuneCount; ++c) {
-    R.candidates[c].warp_row = kTuneCandidates[c].warp_row;
-    R.candidates[c].small_row = kTuneCandidates[c].small_row;
+    R.rows[c][0] = kTuneCandidates[c].warp_row;
+    R.rows[c][1] = kTuneCandidates[c].small_row;
   }
   const uint32_t n_work = g->n_work;
   if (stride == 0) stride = std::max<uint32_t>(1, (uint32_t)(((uint64_t)n_work + kTuneSampleMax - 1) / kTuneSampleMax));
@@ -1028,10 +1032,7 @@ int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report* report) {
       if (R.ms[c] < kTuneMargin * R.ms[0] && R.ms[c] < R.ms[best]) best = c;
   }
   R.best = best;
-  HM_TRY(set_schedule(g, kTuneCandidates[best]));
-  R.tune_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
-  if (report) *report = R;
-  return HM_OK;
+  return set_schedule(g, kTuneCandidates[best], g->tsched);
 }
 
 }  // namespace hm

@@ -58,12 +58,17 @@ class Timings(C.Structure):
 
 
 class Schedule(C.Structure):
-    """Launch split of the closed-triangle phase (hm_schedule)."""
+    """Launch splits of the static and touched-triple counts (hm_schedule)."""
 
-    _fields_ = [("warp_row", C.c_uint32), ("small_row", C.c_uint32)]
+    _fields_ = [
+        ("warp_row", C.c_uint32),
+        ("small_row", C.c_uint32),
+        ("touch_warp_row", C.c_uint32),
+        ("touch_mid_row", C.c_uint32),
+    ]
 
-    def astuple(self) -> tuple[int, int]:
-        return (self.warp_row, self.small_row)
+    def astuple(self) -> tuple[int, int, int, int]:
+        return (self.warp_row, self.small_row, self.touch_warp_row, self.touch_mid_row)
 
 
 TUNE_MAX_CANDIDATES = 16
@@ -75,20 +80,27 @@ class TuneReport(C.Structure):
         ("best", C.c_uint32),
         ("sample_stride", C.c_uint32),
         ("sampled", C.c_uint32),
-        ("candidates", Schedule * TUNE_MAX_CANDIDATES),
+        ("rows", (C.c_uint32 * 2) * TUNE_MAX_CANDIDATES),
         ("ms", C.c_float * TUNE_MAX_CANDIDATES),
+        ("touch_n_candidates", C.c_uint32),
+        ("touch_best", C.c_uint32),
+        ("touch_sampled", C.c_uint32),
+        ("touch_rows", (C.c_uint32 * 2) * TUNE_MAX_CANDIDATES),
+        ("touch_ms", C.c_float * TUNE_MAX_CANDIDATES),
         ("tune_ms", C.c_float),
-        ("pad_", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
-        n = self.n_candidates
+        def part(rows, ms, n, best):
+            return {"best": list(rows[best]), "default": list(rows[0]),
+                    "candidates": [[*rows[i], round(float(ms[i]), 3)] for i in range(n)]}
+
         return {
-            "schedule": list(self.candidates[self.best].astuple()),
-            "default": list(self.candidates[0].astuple()),
-            "sample_stride": self.sample_stride,
-            "sampled_centres": self.sampled,
-            "candidates": [[*self.candidates[i].astuple(), round(float(self.ms[i]), 3)] for i in range(n)],
+            "static": {**part(self.rows, self.ms, self.n_candidates, self.best),
+                       "sample_stride": self.sample_stride, "sampled_centres": self.sampled,
+                       "ms": "closed-phase device time of the sample"},
+            "touch": {**part(self.touch_rows, self.touch_ms, self.touch_n_candidates, self.touch_best),
+                      "sampled_rows": self.touch_sampled, "ms": "wall time of the sample's touched-triple count"},
             "tune_ms": round(float(self.tune_ms), 1),
         }
 
@@ -324,14 +336,19 @@ class Graph:
         return out
 
     @property
-    def schedule(self) -> tuple[int, int]:
-        """(warp_row, small_row) of the closed-phase launch split."""
+    def schedule(self) -> tuple[int, int, int, int]:
+        """(warp_row, small_row, touch_warp_row, touch_mid_row): the launch
+        splits of the static and touched-triple counts."""
         sc = Schedule()
         check(lib.hm_graph_get_schedule(self._h, C.byref(sc)), "hm_graph_get_schedule")
         return sc.astuple()
 
-    def set_schedule(self, warp_row: int, small_row: int) -> None:
-        sc = Schedule(warp_row, small_row)
+    def set_schedule(self, warp_row: int, small_row: int, touch_warp_row: int | None = None,
+                     touch_mid_row: int | None = None) -> None:
+        """Sets the static split; the touched-triple split too when given."""
+        cur = self.schedule
+        sc = Schedule(warp_row, small_row, cur[2] if touch_warp_row is None else touch_warp_row,
+                      cur[3] if touch_mid_row is None else touch_mid_row)
         check(lib.hm_graph_set_schedule(self._h, C.byref(sc)), "hm_graph_set_schedule")
 
     def autotune(self, sample_stride: int = 0) -> TuneReport:
