@@ -407,6 +407,13 @@ typedef struct hm_serve_config {
   uint32_t max_batch_requests; /* requests per round, 0 = no limit */
   uint64_t max_batch_edits;    /* deletions + insertions per round, 0 = no limit */
   size_t mem_budget_bytes;     /* admission budget, 0 = the context's budget */
+  /* 1: once a count request has counted a graph in full, the server keeps
+   * that graph's counts current by adding the exact delta of each of its
+   * updates, and answers its later count requests from them with no device
+   * work; 0: every count request counts its graph in full. The counts are
+   * the same either way. */
+  int32_t count_from_deltas;
+  int32_t pad_;
 } hm_serve_config;
 
 #define HM_REQ_UPDATE 0

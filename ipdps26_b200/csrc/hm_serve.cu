@@ -11,10 +11,13 @@
 //      the static count (open pairs, closed triangles over oriented rows
 //      built for these graphs only) of every queried graph.
 // Update request r gets after[r] - before[r]; count request q gets the static
-// count of its graph. Each graph keeps its
+// count of its graph. With count_from_deltas the server keeps each counted
+// graph's counts current with the deltas of its updates and answers later
+// count requests from them (both forms). Each graph keeps its
 // own ids on the host (smallest free first, like hm_graph_apply_batch) mapped
 // to pool slots, so results match a graph served alone.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -99,6 +102,9 @@ struct hm_server {
   // per-request mode
   std::vector<hm_graph*> graphs;
   std::vector<int> graph_broken;  // per graph: status of a failed update that may have left it half updated
+  // count_from_deltas: per graph, its current 30-class counts once known
+  std::vector<uint8_t> counts_known;
+  std::vector<std::array<uint64_t, 30>> counts;
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -173,6 +179,8 @@ int grow_gos(hm_server* s, uint32_t need) {
 
 int build_stores(hm_server* s) {
   hm_ctx* ctx = s->ctx;
+  s->counts_known.assign(s->staged.size(), 0);
+  s->counts.assign(s->staged.size(), std::array<uint64_t, 30>{});
   if (s->cfg.mode == HM_SERVE_PER_REQUEST) {
     for (auto& st : s->staged) {
       auto* g = new hm_graph();
@@ -245,6 +253,18 @@ void finish(hm_server* s, Request& r, int status) {
   r.res.done_ms = now_ms(s->t0);
 }
 
+// A count request that needs a full count (no counts kept for its graph).
+bool counts_in_full(const hm_server* s, const Request& r) {
+  return r.kind == HM_REQ_COUNT && !(s->cfg.count_from_deltas && s->counts_known[r.graph]);
+}
+
+// The exact delta of an update of graph k, added to its known counts
+// (modulo 2^64, as the counts are uint64).
+void add_delta(hm_server* s, uint32_t k, const int64_t delta30[30]) {
+  if (!s->cfg.count_from_deltas || !s->counts_known[k]) return;
+  for (int c = 0; c < 30; ++c) s->counts[k][c] += (uint64_t)delta30[c];
+}
+
 // One request on its own store (the plain per-call form). An update that
 // fails for another reason than its own arguments (which are checked before
 // the store changes) may have left the graph half updated: the graph then
@@ -258,7 +278,16 @@ void serve_one(hm_server* s, Request& r) {
   }
   int rc;
   if (r.kind == HM_REQ_COUNT) {
-    rc = count_static30(g, 0, 1, r.res.counts30);
+    if (s->cfg.count_from_deltas && s->counts_known[r.graph]) {
+      std::memcpy(r.res.counts30, s->counts[r.graph].data(), sizeof(r.res.counts30));
+      rc = HM_OK;
+    } else {
+      rc = count_static30(g, 0, 1, r.res.counts30);
+      if (rc >= 0 && s->cfg.count_from_deltas) {
+        std::memcpy(s->counts[r.graph].data(), r.res.counts30, sizeof(r.res.counts30));
+        s->counts_known[r.graph] = 1;
+      }
+    }
   } else {
     const uint32_t n_ins = r.n_ins();
     r.assigned.resize(n_ins);
@@ -267,6 +296,7 @@ void serve_one(hm_server* s, Request& r) {
                      n_ins, r.assigned.data(), r.res.delta30);
     r.res.n_assigned = n_ins;
     if (rc < 0 && rc != HM_ERR_INVALID && rc != HM_ERR_NOT_LIVE && rc != HM_ERR_LIMIT) broken = rc;
+    if (rc >= 0) add_delta(s, r.graph, r.res.delta30);
   }
   finish(s, r, rc < 0 ? rc : HM_OK);
 }
@@ -303,6 +333,12 @@ void serve_round(hm_server* s, std::vector<ReqPtr>& batch) {
         ins_graph.push_back(r.graph);
       }
     } else {
+      if (s->cfg.count_from_deltas && s->counts_known[r.graph]) {
+        // the graph's earlier requests were served in earlier rounds
+        std::memcpy(r.res.counts30, s->counts[r.graph].data(), sizeof(r.res.counts30));
+        finish(s, r, HM_OK);
+        continue;
+      }
       for (uint32_t slot : gi.slot_of_id)
         if (slot != kNone) qslots.push_back(slot);
     }
@@ -370,8 +406,13 @@ void serve_round(hm_server* s, std::vector<ReqPtr>& batch) {
     const uint64_t* b = before.data() + (size_t)row * 30;
     if (r.kind == HM_REQ_COUNT) {
       std::memcpy(r.res.counts30, full.data() + (size_t)row * 30, sizeof(r.res.counts30));
+      if (s->cfg.count_from_deltas) {
+        std::memcpy(s->counts[r.graph].data(), r.res.counts30, sizeof(r.res.counts30));
+        s->counts_known[r.graph] = 1;
+      }
     } else {
       for (int k = 0; k < 30; ++k) r.res.delta30[k] = (int64_t)(a[k] - b[k]);
+      add_delta(s, r.graph, r.res.delta30);
       GraphIds& gi = s->ids[r.graph];
       for (uint32_t d : r.dels) {
         gi.slot_of_id[d] = kNone;
@@ -422,7 +463,7 @@ std::vector<ReqPtr> select_round(hm_server* s) {
     }
     seen[r.graph] = 1;
     const uint64_t e = r.edits();
-    const uint64_t m = r.kind == HM_REQ_COUNT ? s->ids[r.graph].n_live : 0;
+    const uint64_t m = counts_in_full(s, r) ? s->ids[r.graph].n_live : 0;
     bool take = true;
     if (s->cfg.max_batch_requests && out.size() >= s->cfg.max_batch_requests) take = false;
     if (take && s->cfg.max_batch_edits && !out.empty() && edits + e > s->cfg.max_batch_edits) take = false;
@@ -464,7 +505,7 @@ void loop_main(hm_server* s) {
         for (auto& r : batch) {
           // a request that cannot fit the budget alone fails before any device work
           const hm_graph* g = s->graphs[r->graph];
-          const size_t est = round_estimate(g, r->edits(), r->kind == HM_REQ_COUNT ? g->n_live : 0);
+          const size_t est = round_estimate(g, r->edits(), counts_in_full(s, *r) ? g->n_live : 0);
           if (s->ctx->used.load() + est > s->budget())
             finish(s, *r, set_error(HM_ERR_NOMEM, "serve: the request does not fit the memory budget"));
           else
@@ -474,7 +515,7 @@ void loop_main(hm_server* s) {
         bool fits = true;
         if (batch.size() == 1) {  // a request admitted alone must still fit
           Request& r = *batch[0];
-          const uint64_t m = r.kind == HM_REQ_COUNT ? s->ids[r.graph].n_live : 0;
+          const uint64_t m = counts_in_full(s, r) ? s->ids[r.graph].n_live : 0;
           if (s->ctx->used.load() + round_estimate(s->pool, r.edits(), m) > s->budget()) {
             finish(s, r, set_error(HM_ERR_NOMEM, "serve: the request does not fit the memory budget"));
             fits = false;
@@ -532,6 +573,10 @@ extern "C" int hm_serve_create(hm_ctx* ctx, const hm_serve_config* cfg, hm_serve
   if (s->cfg.mode != HM_SERVE_BATCHED && s->cfg.mode != HM_SERVE_PER_REQUEST) {
     delete s;
     return hm::set_error(HM_ERR_INVALID, "hm_serve_create: unknown mode %d", (int)cfg->mode);
+  }
+  if (s->cfg.count_from_deltas != 0 && s->cfg.count_from_deltas != 1) {
+    delete s;
+    return hm::set_error(HM_ERR_INVALID, "hm_serve_create: count_from_deltas must be 0 or 1");
   }
   *out = s;
   return HM_OK;

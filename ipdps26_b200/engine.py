@@ -111,6 +111,8 @@ class ServeConfig(C.Structure):
         ("max_batch_requests", C.c_uint32),
         ("max_batch_edits", C.c_uint64),
         ("mem_budget_bytes", C.c_size_t),
+        ("count_from_deltas", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 
@@ -477,8 +479,8 @@ class Server:
     """
 
     def __init__(self, ctx: Context, mode: int = SERVE_BATCHED, max_batch_requests: int = 0,
-                 max_batch_edits: int = 0, mem_budget_bytes: int = 0):
-        cfg = ServeConfig(mode, max_batch_requests, max_batch_edits, mem_budget_bytes)
+                 max_batch_edits: int = 0, mem_budget_bytes: int = 0, count_from_deltas: bool = False):
+        cfg = ServeConfig(mode, max_batch_requests, max_batch_edits, mem_budget_bytes, int(count_from_deltas))
         h = vp()
         check(lib.hm_serve_create(ctx.handle, C.byref(cfg), C.byref(h)), "hm_serve_create")
         self._h = h

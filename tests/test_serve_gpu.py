@@ -1,6 +1,7 @@
 """Served requests over many resident graphs (hm_serve_*): every result is the
-same in the batched mix, in the per-request form and on the graph alone, and
-final counts match the oracle."""
+same in the batched mix, in the per-request form and on the graph alone, with
+and without counts kept current by the exact deltas, and final counts match
+the oracle."""
 import numpy as np
 import pytest
 
@@ -243,3 +244,45 @@ def test_failed_round_is_reported_and_later_requests_fail_cleanly(ctx, mode):
             assert r3.status == 0  # graph 2 has its own store
             with engine.Graph.from_hypergraph(ctx, hs[2]) as g:
                 assert list(r3.counts30) == g.count_static30().tolist()
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_counts_from_deltas_equal_full_counts(ctx, seed):
+    """count_from_deltas: counts kept current by the exact deltas answer the
+    later count requests of each graph; every result equals the plain form,
+    which counts in full every time."""
+    from ipdps26_b200 import engine, serve_trace
+
+    ps, hs = _graphs(small=(seed == 1))
+    trace = _trace(ps, 90, seed)
+    final = [serve_trace.Request(1e9, k, engine.REQ_COUNT) for k in range(len(hs))]
+    full, live_f, _ = _run(ctx, hs, trace + final, engine.SERVE_PER_REQUEST)
+    assert sum(r.kind == engine.REQ_COUNT for r in trace) > len(hs)  # graphs counted more than once
+    for mode in (engine.SERVE_BATCHED, engine.SERVE_PER_REQUEST):
+        kept, live_k, _ = _run(ctx, hs, trace + final, mode, count_from_deltas=True)
+        assert all(r.status == 0 for r, _ in kept.results)
+        assert serve_trace.same_results(full, kept), mode
+        assert all(np.array_equal(a, b) for a, b in zip(live_f, live_k))
+
+
+def test_counts_from_deltas_survive_rejected_updates(ctx):
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HM_ERR_NOT_LIVE
+
+    ps, hs = _graphs(small=True)
+    off, mem = np.array([0, 3], np.uint64), np.array([1, 2, 3], np.uint32)
+    for mode in (engine.SERVE_BATCHED, engine.SERVE_PER_REQUEST):
+        with engine.Server(ctx, mode, count_from_deltas=True) as s:
+            for h in hs:
+                s.add_graph(h.offsets, h.members, h.n_nodes)
+            s.start()
+            r0, _ = s.wait(s.submit_count(0))
+            bad, _ = s.wait(s.submit_update(0, [hs[0].n_edges + 5]))
+            ok, _ = s.wait(s.submit_update(0, [0], off, mem))
+            r1, _ = s.wait(s.submit_count(0))
+        assert bad.status == HM_ERR_NOT_LIVE and ok.status == 0
+        with engine.Graph.from_hypergraph(ctx, hs[0]) as g:
+            assert list(r0.counts30) == g.count_static30().tolist()
+            _, d = g.apply_batch([0], off, mem)
+            assert list(ok.delta30) == d.tolist()
+            assert list(r1.counts30) == g.count_static30().tolist()
