@@ -354,9 +354,7 @@ def engine_arm(args, rank, world, local_rank):
         if rank == 0:
             tune = g.autotune(args.tune_stride).as_dict()
         if world > 1:
-            sched = torch.tensor(list(g.schedule), dtype=torch.int64, device=f"cuda:{local_rank}")
-            dist.broadcast(sched, 0)
-            g.set_schedule(*[int(x) for x in sched.tolist()])
+            g.set_schedule(*shard.agree_schedule(g.schedule, dist, f"cuda:{local_rank}"))
 
     def step():
         part = g.count_static30_shard(rank, world)

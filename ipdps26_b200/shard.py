@@ -40,6 +40,21 @@ def max_over_ranks(seconds: float, dist, device=None) -> float:
     return float(t.item())
 
 
+def agree_schedule(schedule, dist, device=None, src: int = 0) -> tuple[int, ...]:
+    """Every rank's copy of rank `src`'s launch schedule.
+
+    The GPU shards take every world-th item of one heaviest-first work list,
+    and the order of that list follows the schedule (it is split into the
+    launch shapes first), so the partials add up to the full count only when
+    all ranks use the same schedule: tune on one rank, then agree on it.
+    """
+    import torch
+
+    t = torch.tensor([int(x) for x in schedule], dtype=torch.int64, device=device)
+    dist.broadcast(t, src)
+    return tuple(int(x) for x in t.cpu().tolist())
+
+
 def owner_shard(owner_ids: np.ndarray, world: int) -> np.ndarray:
     """Rank that counts the triples of each owner id under the round-robin
     split the oracle shard uses (a mod world)."""

@@ -44,6 +44,9 @@ def _rank_main(rank, world, port, cases, out_dir):
         big = np.array([2**63 + 5, 2**64 - 1 - rank, 7], np.uint64)
         res["big"] = (big, shard.allreduce_counts(big, dist))
         res["max"] = shard.max_over_ranks(1.5 + rank, dist)
+        # each rank tuned its own schedule; rank 0's is the one all use
+        mine = (64, 2048, 0, 1024) if rank == 0 else (128, 2048, 128, 2048)
+        res["schedule"] = shard.agree_schedule(mine, dist)
         np.save(os.path.join(out_dir, f"rank{rank}.npy"), np.array([res], dtype=object), allow_pickle=True)
     finally:
         dist.destroy_process_group()
@@ -79,6 +82,7 @@ def test_sharded_count_all_reduce_over_gloo(tmp_path):
     for r in range(WORLD):
         assert np.array_equal(results[r]["big"][1], want_big)
         assert results[r]["max"] == pytest.approx(1.5 + WORLD - 1)
+        assert results[r]["schedule"] == (64, 2048, 0, 1024)
 
 
 def test_owner_shards_cover_every_owner_once():
