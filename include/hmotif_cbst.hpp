@@ -140,6 +140,21 @@ class HypergraphStore {
     return out;
   }
 
+  // Launch schedules of the two counts (no reference counterpart): tune
+  // once after construct, or apply a schedule tuned on a graph of the same
+  // shape. Counts do not depend on them.
+  hm_tune_report autotune(uint32_t sample_stride = 0) {
+    hm_tune_report r{};
+    check(hm_graph_autotune(g_, sample_stride, &r), "hm_graph_autotune");
+    return r;
+  }
+  hm_schedule schedule() const {
+    hm_schedule s{};
+    check(hm_graph_get_schedule(g_, &s), "hm_graph_get_schedule");
+    return s;
+  }
+  void set_schedule(const hm_schedule& s) { check(hm_graph_set_schedule(g_, &s), "hm_graph_set_schedule"); }
+
   hm_graph* context() const { return g_; }
 
  private:

@@ -71,6 +71,7 @@ def test_cpp_shim_compiles_and_links(tmp_path):
         "  hm::HypergraphStore s(ctx, \"H2V\");\n"
         "  int starts[2] = {0, 4}; int flat[8] = {1, 2, 0, 0, 2, 3, 0, 0};\n"
         "  s.construct(starts, 2, flat, 8, 4);\n"
+        "  s.set_schedule(s.autotune().best ? s.schedule() : hm_schedule{128, 2048, 128, 2048});\n"
         "  auto c = hm::computeMotifCounts(s);\n"
         "  std::vector<int64_t> d; s.update({1}, {1, 3}, {2}, &d);\n"
         "  s.findAndPrint({1, 2});\n"
