@@ -14,6 +14,16 @@
 // change of the counts. payload_capacity and alignment are accepted for
 // compatibility; the store has no fixed capacity.
 //
+// The temporal driver's flags (temporalDynamicHMotif/src/main.cu:262-372,
+// utils/utils.cpp:13-40): --temporal counts the strictly increasing 30
+// classes of a three-layer window whose layers all hold the graph, then of
+// the window whose newest layer holds the graph after the batch, and prints
+// the first counts and the difference; --temporal-synthetic uses the
+// reference's fixed three-hyperedge window instead; --temporal-deltas=PATH
+// applies "A|R <hyperedge> <vertices>" lines to the newer window's newest
+// layer (in generate/input mode after rotating the older window so that its
+// newest layer holds the graph after the batch too).
+//
 // Additions: --input-dir=DIR (default input, as the reference),
 // --input-format=escher|mochy|thyme, --seed=S (the reference seeds with the
 // time), --mochy (print MoCHy's 26 motifs as "motif i: c"),
@@ -44,6 +54,8 @@ struct Args {
   unsigned long long seed = 0;
   bool mochy = false, no_update = false;
   long long temporal_delta = -1;
+  bool temporal = false, temporal_synthetic = false;
+  std::string temporal_deltas;
   int device = 0;
 };
 
@@ -55,7 +67,7 @@ void usage(const char* prog) {
                "Usage (input mode):    %s <payload_capacity> [alignment=4] --input=FILE [-totalChanges N] "
                "[-insertionPercentage P] [-deletionPercentage P]\n"
                "Options: --input-dir=DIR --input-format=escher|mochy|thyme --seed=S --mochy --temporal-delta=D "
-               "--device=N --no-update\n",
+               "--temporal [--temporal-synthetic] [--temporal-deltas=PATH] --device=N --no-update\n",
                prog, prog);
 }
 
@@ -149,6 +161,12 @@ int parse(int argc, char** argv, Args& a) {
       a.mochy = true;
     } else if (s == "--no-update") {
       a.no_update = true;
+    } else if (s == "--temporal") {
+      a.temporal = true;
+    } else if (s == "--temporal-synthetic") {
+      a.temporal_synthetic = true;
+    } else if (s.rfind("--temporal-deltas=", 0) == 0) {
+      a.temporal_deltas = s.substr(18);
     } else if (s.rfind("--temporal-delta=", 0) == 0) {
       long long d;
       if (!pos_int(s.substr(17), d)) {
@@ -209,6 +227,10 @@ int parse(int argc, char** argv, Args& a) {
     std::fprintf(stderr, "Error: --temporal-delta needs --input-format=thyme\n");
     return 1;
   }
+  if (a.temporal && a.temporal_delta > 0) {
+    std::fprintf(stderr, "Error: --temporal (three-layer window) and --temporal-delta (THyMe) exclude each other\n");
+    return 1;
+  }
   return 0;
 }
 
@@ -235,6 +257,75 @@ int fail(const char* what) {
 void print30(const char* title, const uint64_t* c) {
   std::printf("%s (30 bins): ", title);
   for (int i = 0; i < HM_N_STATIC_CLASSES; ++i) std::printf("%llu%c", (unsigned long long)c[i], i + 1 < 30 ? ' ' : '\n');
+}
+
+using Rows = std::vector<std::vector<uint32_t>>;
+
+int set_layer(hm_window* w, int layer, const Rows& rows) {
+  std::vector<uint64_t> off(1, 0);
+  std::vector<uint32_t> mem;
+  for (const auto& r : rows) {
+    mem.insert(mem.end(), r.begin(), r.end());
+    off.push_back(mem.size());
+  }
+  return hm_window_set_layer(w, layer, off.data(), mem.data(), (uint32_t)rows.size());
+}
+
+// The three-layer strictly increasing count of the temporal driver. base is
+// the graph, updated the graph after the batch (deleted rows empty, inserted
+// rows at their ids); the synthetic window replaces both.
+int temporal_windows(const Args& a, hm_ctx* ctx, uint32_t n_nodes, const Rows& base, const Rows& updated) {
+  // the reference's fixed window: Older = Middle = Newest = {1,2},{2,3},{1,3};
+  // the newer window's Newest is {1,2},{2,3},{1,2,3} (vertex v is node v - 1)
+  const Rows syn = {{0, 1}, {1, 2}, {0, 2}}, syn_new = {{0, 1}, {1, 2}, {0, 1, 2}};
+  const uint32_t wn = std::max<uint32_t>(n_nodes, 3);
+  hm_window *ow = nullptr, *nw = nullptr;
+  if (hm_window_create(ctx, wn, &ow) < 0 || hm_window_create(ctx, wn, &nw) < 0) {
+    hm_window_destroy(ow);
+    return fail("creating the temporal windows");
+  }
+  int rc = 0;
+  uint64_t c_old[HM_N_STATIC_CLASSES], c_new[HM_N_STATIC_CLASSES];
+  const Rows& older = a.temporal_synthetic ? syn : base;
+  const Rows& newest = a.temporal_synthetic ? syn_new : updated;
+  do {
+    if (set_layer(ow, HM_LAYER_OLDER, older) < 0 || set_layer(ow, HM_LAYER_MIDDLE, older) < 0 ||
+        set_layer(ow, HM_LAYER_NEWEST, older) < 0) {
+      rc = fail("building the older window");
+      break;
+    }
+    if (hm_window_count30(ow, c_old) < 0) {
+      rc = fail("temporal count");
+      break;
+    }
+    print30("Temporal strict-inc counts", c_old);
+    if (set_layer(nw, HM_LAYER_OLDER, older) < 0 || set_layer(nw, HM_LAYER_MIDDLE, older) < 0 ||
+        set_layer(nw, HM_LAYER_NEWEST, newest) < 0) {
+      rc = fail("building the newer window");
+      break;
+    }
+    if (!a.temporal_deltas.empty()) {
+      if (!a.temporal_synthetic &&
+          (hm_window_rotate(ow) < 0 || set_layer(ow, HM_LAYER_NEWEST, updated) < 0 || hm_window_count30(ow, c_old) < 0)) {
+        rc = fail("rotating the older window");
+        break;
+      }
+      if (hm_window_apply_deltas_file(nw, a.temporal_deltas.c_str()) < 0) {
+        rc = fail("applying the temporal deltas");
+        break;
+      }
+    }
+    if (hm_window_count30(nw, c_new) < 0) {
+      rc = fail("temporal count");
+      break;
+    }
+    std::printf("Temporal strict-inc delta (30 bins): ");
+    for (int i = 0; i < HM_N_STATIC_CLASSES; ++i)
+      std::printf("%lld%c", (long long)(c_new[i] - c_old[i]), i + 1 < 30 ? ' ' : '\n');
+  } while (false);
+  hm_window_destroy(ow);
+  hm_window_destroy(nw);
+  return rc;
 }
 
 }  // namespace
@@ -303,6 +394,9 @@ int main(int argc, char** argv) {
     hm_ctx_destroy(ctx);
     return 0;
   }
+  Rows base(n_edges);
+  for (uint32_t e = 0; e < n_edges; ++e) base[e].assign(mem.begin() + off[e], mem.begin() + off[e + 1]);
+  Rows updated = base;
   if (hm_graph_build(ctx, off.data(), mem.data(), n_edges, n_nodes, nullptr, &g) < 0) return fail("build");
   uint64_t c30[HM_N_STATIC_CLASSES];
   if (hm_count_static30(g, c30) < 0) return fail("count");
@@ -343,11 +437,17 @@ int main(int argc, char** argv) {
       return fail("update batch");
     std::printf("Inserted ids (1-based):");
     for (long long i = 0; i < n_ins; ++i) std::printf(" %u", ids[i] + 1);
+    for (uint32_t d : dels) updated[d].clear();
+    for (long long i = 0; i < n_ins; ++i) {
+      if (ids[i] >= updated.size()) updated.resize(ids[i] + 1);
+      updated[ids[i]].assign(imem.begin() + ioff[i], imem.begin() + ioff[i + 1]);
+    }
     std::printf("\nMotif delta counts (30 bins): ");
     for (int i = 0; i < HM_N_STATIC_CLASSES; ++i) std::printf("%lld%c", (long long)d30[i], i + 1 < 30 ? ' ' : '\n');
     if (hm_count_static30(g, c30) < 0) return fail("count");
     print30("Motif counts after the batch", c30);
   }
+  if (a.temporal) rc = temporal_windows(a, ctx, n_nodes, base, updated);
   hm_graph_destroy(g);
   hm_ctx_destroy(ctx);
   return rc;
