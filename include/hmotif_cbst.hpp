@@ -9,7 +9,12 @@
 //     here also returns the counts (30 bins, the reference's order) instead of
 //     only printing them;
 //   * computeMotifCountsDelta (dynamicHyperGraph/include/motif_update.hpp:
-//     13-19) as one call that applies the batch and returns the exact change.
+//     13-19) as one call that applies the batch and returns the exact change;
+//   * the temporal ring of three layers (TemporalCBSTOperations /
+//     TemporalHypergraphIndex, temporalDynamicHMotif/include/
+//     temporal_structure.hpp:22-80, temporal_adjacency.hpp:9-19) and
+//     computeTemporalMotifCountsStrictInc / ...Delta /
+//     applyTemporalDeltasFromFile (include/temporal_count.hpp:10-30).
 // One HypergraphStore holds H2V, V2H and H2H together; the reference needs
 // three CBSTOperations for that. Errors throw hm::Error (the reference calls
 // exit(-1)).
@@ -174,6 +179,115 @@ inline std::vector<uint64_t> computeMotifCounts(const HypergraphStore& store, bo
       std::printf("%llu%c", (unsigned long long)c[i], i + 1 < HM_N_STATIC_CLASSES ? ' ' : '\n');
   }
   return c;
+}
+
+// Logical layers of the temporal ring (temporal_structure.hpp:20).
+enum class TemporalLayer { Older = HM_LAYER_OLDER, Middle = HM_LAYER_MIDDLE, Newest = HM_LAYER_NEWEST };
+
+// The reference's three-layer ring on one hm_window: the H2V side of each
+// layer (V2H follows by itself). Keys are the layer's 1-based hyperedge ids;
+// vertex v is node v - 1, as in the delta files. The reference's
+// per-layer insert / erase of whole records has no counterpart here: a
+// layer is rebuilt with construct.
+class TemporalWindow {
+ public:
+  // max_vertex: the largest vertex id any layer will hold.
+  TemporalWindow(Context& ctx, uint32_t max_vertex) {
+    check(hm_window_create(ctx.get(), max_vertex, &w_), "hm_window_create");
+  }
+  ~TemporalWindow() { hm_window_destroy(w_); }
+  TemporalWindow(const TemporalWindow&) = delete;
+  TemporalWindow& operator=(const TemporalWindow&) = delete;
+
+  // construct(layer, ...) (temporal_structure.hpp:34-39): record i has key
+  // cbstKeys[i] (1-based) and starts at cbstStartOffsets[i]; it ends at a
+  // 0 pad, a negative value or the next record's start. Keys left out are
+  // empty hyperedges. Replaces what the layer held.
+  void construct(TemporalLayer layer, const int* cbstKeys, const int* cbstStartOffsets, int numRecords,
+                 const int* flatPayload, int flatPayloadSize) {
+    std::vector<std::vector<uint32_t>> rows;
+    for (int i = 0; i < numRecords; ++i) {
+      const int key = cbstKeys ? cbstKeys[i] : i + 1;
+      if (key < 1) throw std::invalid_argument("TemporalWindow::construct: keys are 1-based");
+      if ((int)rows.size() < key) rows.resize(key);
+      const int end = (i + 1 < numRecords) ? cbstStartOffsets[i + 1] : flatPayloadSize;
+      for (int k = cbstStartOffsets[i]; k < end; ++k) {
+        const int v = flatPayload[k];
+        if (v <= 0) break;
+        rows[key - 1].push_back((uint32_t)(v - 1));
+      }
+    }
+    std::vector<uint64_t> off(1, 0);
+    std::vector<uint32_t> mem;
+    for (const auto& r : rows) {
+      mem.insert(mem.end(), r.begin(), r.end());
+      off.push_back(mem.size());
+    }
+    check(hm_window_set_layer(w_, (int)layer, off.data(), mem.data(), (uint32_t)rows.size()), "hm_window_set_layer");
+  }
+
+  // fill / unfill (fillCBST / unfillCBST): vertices added to or removed from
+  // existing hyperedges; prefix[i] is the inclusive end of keys[i]'s values.
+  void fill(TemporalLayer layer, const std::vector<int>& keys, const std::vector<int>& payload,
+            const std::vector<int>& prefix) {
+    edit(layer, keys, payload, prefix, false);
+  }
+  void unfill(TemporalLayer layer, const std::vector<int>& keys, const std::vector<int>& valuesToRemove,
+              const std::vector<int>& removePrefix) {
+    edit(layer, keys, valuesToRemove, removePrefix, true);
+  }
+
+  // rotate (Middle becomes Older, Newest Middle, Older Newest) and resets.
+  void rotate() { check(hm_window_rotate(w_), "hm_window_rotate"); }
+  void resetLayer(TemporalLayer layer) { check(hm_window_reset_layer(w_, (int)layer), "hm_window_reset_layer"); }
+  void resetNewest() { resetLayer(TemporalLayer::Newest); }
+
+  uint32_t size(TemporalLayer layer) const {
+    uint32_t n = 0;
+    check(hm_window_layer_size(w_, (int)layer, &n), "hm_window_layer_size");
+    return n;
+  }
+  hm_window* get() const { return w_; }
+
+ private:
+  void edit(TemporalLayer layer, const std::vector<int>& keys, const std::vector<int>& values,
+            const std::vector<int>& prefix, bool remove) {
+    if (keys.size() != prefix.size()) throw std::invalid_argument("TemporalWindow: one prefix end per key");
+    std::vector<uint32_t> ids, vals;
+    for (int k : keys) ids.push_back((uint32_t)(k - 1));
+    for (int v : values) vals.push_back((uint32_t)(v - 1));
+    std::vector<uint64_t> ends(prefix.begin(), prefix.end());
+    const int s = remove ? hm_window_unfill(w_, (int)layer, ids.data(), (uint32_t)ids.size(), vals.data(), ends.data())
+                         : hm_window_fill(w_, (int)layer, ids.data(), (uint32_t)ids.size(), vals.data(), ends.data());
+    check(s, remove ? "hm_window_unfill" : "hm_window_fill");
+  }
+
+  hm_window* w_ = nullptr;
+};
+
+// computeTemporalMotifCountsStrictInc (temporal_count.hpp:10-16): the 30
+// classes of the closed triples (i Older, j Middle, k Newest, i < j < k),
+// without the reference's cap of 1024 candidates per middle hyperedge.
+inline void computeTemporalMotifCountsStrictInc(const TemporalWindow& w, std::vector<int64_t>& outCounts30) {
+  std::vector<uint64_t> c(HM_N_STATIC_CLASSES);
+  check(hm_window_count30(w.get(), c.data()), "hm_window_count30");
+  outCounts30.assign(c.begin(), c.end());
+}
+
+// computeTemporalMotifCountsStrictIncDelta: counts(newWindow) - counts(oldWindow).
+inline void computeTemporalMotifCountsStrictIncDelta(const TemporalWindow& oldWindow, const TemporalWindow& newWindow,
+                                                     std::vector<int64_t>& outDeltaCounts30) {
+  std::vector<int64_t> a, b;
+  computeTemporalMotifCountsStrictInc(oldWindow, a);
+  computeTemporalMotifCountsStrictInc(newWindow, b);
+  outDeltaCounts30.assign(HM_N_STATIC_CLASSES, 0);
+  for (int i = 0; i < HM_N_STATIC_CLASSES; ++i) outDeltaCounts30[i] = b[i] - a[i];
+}
+
+// applyTemporalDeltasFromFile: "A|R <hyperedge> <vertices>" lines on the
+// Newest layer; false (and nothing changed) on a bad file.
+inline bool applyTemporalDeltasFromFile(const std::string& path, TemporalWindow& w) {
+  return hm_window_apply_deltas_file(w.get(), path.c_str()) == HM_OK;
 }
 
 // MoCHy's 26 motifs (MoCHy-master/main_exact.cpp:133-137), 1-based "motif i".

@@ -75,6 +75,17 @@ def test_cpp_shim_compiles_and_links(tmp_path):
         "  auto c = hm::computeMotifCounts(s);\n"
         "  std::vector<int64_t> d; s.update({1}, {1, 3}, {2}, &d);\n"
         "  s.findAndPrint({1, 2});\n"
+        "  hm::TemporalWindow w(ctx, 3), w2(ctx, 3);\n"
+        "  int keys[3] = {1, 2, 3}, st[3] = {0, 2, 4}, L[6] = {1, 2, 2, 3, 1, 3};\n"
+        "  for (auto l : {hm::TemporalLayer::Older, hm::TemporalLayer::Middle, hm::TemporalLayer::Newest})\n"
+        "    w.construct(l, keys, st, 3, L, 6);\n"
+        "  w.fill(hm::TemporalLayer::Newest, {3}, {2}, {1});\n"
+        "  w.unfill(hm::TemporalLayer::Newest, {3}, {1}, {1});\n"
+        "  w.rotate(); w.resetNewest();\n"
+        "  bool ok = hm::applyTemporalDeltasFromFile(\"d.txt\", w2) && w.size(hm::TemporalLayer::Older) == 3;\n"
+        "  std::vector<int64_t> t; hm::computeTemporalMotifCountsStrictIncDelta(w, w2, t);\n"
+        "  hm::computeTemporalMotifCountsStrictInc(w, t);\n"
+        "  if (!ok) return 3;\n"
         "  return (int)c[0];\n"
         "}\n")
     out = tmp_path / "use_shim"
