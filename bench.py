@@ -461,6 +461,7 @@ def engine_arm(args, rank, world, local_rank):
             "config": {**config_of(args, world), "schedule": list(g_sched)}, "gpu_launches": 4 * args.steps,
             "autotune": tune,
             "triples_per_step": triples, "closed_triangles_per_step": closed_tri,
+            "closed_triangles_per_s": closed_tri * args.steps / dev_s,
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
                       "device_gb": info.device_bytes / 1e9},
