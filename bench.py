@@ -387,6 +387,8 @@ def engine_arm(args, rank, world, local_rank):
     dev_s = e0.elapsed_time(e1) / 1000.0
     if world > 1:
         dev_s = shard.max_over_ranks(dev_s, dist, f"cuda:{local_rank}")
+        # each rank enumerated the closed triangles of its own shard
+        closed_tri = int(shard.allreduce_counts(np.array([closed_tri], np.uint64), dist, f"cuda:{local_rank}")[0])
     triples = int(counts.astype(np.uint64).sum())
     value = triples * args.steps / dev_s
 
