@@ -475,7 +475,10 @@ class Server:
 
     ``mode`` SERVE_BATCHED serves one request of every waiting graph per
     round over a pooled store; SERVE_PER_REQUEST serves them one call at a
-    time on per-graph stores. Results are the same.
+    time on per-graph stores. With ``count_from_deltas`` a graph's counts,
+    once counted in full, are kept current by the exact deltas of its
+    updates and answer its later count requests. Results are the same in
+    every form.
     """
 
     def __init__(self, ctx: Context, mode: int = SERVE_BATCHED, max_batch_requests: int = 0,
