@@ -248,6 +248,16 @@ int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_M
  * single 30 x uint64 sum across ranks. */
 int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[HM_N_STATIC_CLASSES]);
 
+/* The 30-class static count, asynchronous: queued after the work already on
+ * `stream` (a cudaStream_t; NULL: the context stream), it writes the counts
+ * to d_out30 (device memory, 30 uint64) and returns without waiting; work
+ * queued on `stream` afterwards sees them. The first call on a graph (and
+ * the first after an update) prepares the oriented rows and the work list
+ * and waits for that. Do not change the graph or count it again until the
+ * stream has passed the count. The reference's calls all end in a device
+ * synchronize (dynamicHyperGraph/src/HMotifCount.cu:97-125). */
+int hm_count_static30_async(hm_graph* g, uint64_t* d_out30, void* stream);
+
 /* Algorithmic bytes of one static count of this graph (for rooflines):
  * b_static follows the reference-equivalent merge algorithm
  * (MoCHy-master/main_exact.cpp:91-129): store read once

@@ -134,6 +134,13 @@ extern "C" int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_s
   return hm::count_static30(g, shard, n_shards, out30);
 }
 
+extern "C" int hm_count_static30_async(hm_graph* g, uint64_t* d_out30, void* stream) {
+  if (!g || !d_out30) return hm::set_error(HM_ERR_INVALID, "hm_count_static30_async: NULL argument");
+  HM_TRY(static_ok(g));
+  CtxLock lock(g->ctx);
+  return hm::count_static30_async(g, d_out30, static_cast<cudaStream_t>(stream));
+}
+
 extern "C" int hm_graph_set_schedule(hm_graph* g, const hm_schedule* s) {
   if (!g || !s) return hm::set_error(HM_ERR_INVALID, "hm_graph_set_schedule: NULL argument");
   CtxLock lock(g->ctx);

@@ -239,6 +239,7 @@ int prepare_static(hm_graph* g);
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags);
 int finish_static(hm_graph* g, uint64_t out30[30]);
 int count_static30(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[30]);
+int count_static30_async(hm_graph* g, uint64_t* d_out30, cudaStream_t user);
 int count_vertex_triads(hm_graph* g, uint64_t out3[3]);
 int set_schedule(hm_graph* g, const ClosedSchedule& s, const TouchSchedule& t);
 // The autotuner's two parts: static count (hm_static.cu), touched-triple

@@ -757,6 +757,54 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   return HM_OK;
 }
 
+namespace {
+// The 30 classes from the counter block: closed classes, plus the open-pair
+// counts minus the removals closed triangles made (as finish_static).
+__global__ void k_finish30(const unsigned long long* c, uint64_t* out30) {
+  const unsigned k = threadIdx.x;
+  if (k < 30) out30[k] = c[k] + (k >= 20 && k < 26 ? c[36 + k - 20] - c[30 + k - 20] : 0ull);
+}
+}  // namespace
+
+// One count queued after `user` (the context stream when null), its classes
+// written to d_out30, no host wait once the graph is prepared.
+int count_static30_async(hm_graph* g, uint64_t* d_out30, cudaStream_t user) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  HM_TRY(prepare_static(g));
+  const bool other = user && user != st;
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  auto release = [&]() {
+    for (auto x : e)
+      if (x) cudaEventDestroy(x);  // released once the recorded work completes
+  };
+  if (other) {
+    cudaError_t r = cudaEventCreateWithFlags(&e[0], cudaEventDisableTiming);
+    if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e[1], cudaEventDisableTiming);
+    if (r == cudaSuccess) r = cudaEventRecord(e[0], user);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(st, e[0], 0);
+    if (r != cudaSuccess) {
+      release();
+      return set_error(HM_ERR_CUDA, "async static count: ordering after the caller's stream: %s",
+                       cudaGetErrorString(r));
+    }
+  }
+  int rc = launch_static(g, 0, 1, nullptr);
+  if (rc >= 0) {
+    k_finish30<<<1, 32, 0, st>>>(g->counters.p, d_out30);
+    const cudaError_t r = cudaGetLastError();
+    if (r != cudaSuccess) rc = set_error(HM_ERR_CUDA, "async static count: %s", cudaGetErrorString(r));
+  }
+  if (rc >= 0 && other) {
+    cudaError_t r = cudaEventRecord(e[1], st);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(user, e[1], 0);
+    if (r != cudaSuccess) rc = set_error(HM_ERR_CUDA, "async static count: ordering the caller's stream: %s",
+                                         cudaGetErrorString(r));
+  }
+  release();
+  return rc;
+}
+
 int finish_static(hm_graph* g, uint64_t out30[30]) {
   unsigned long long h[44];
   cudaStream_t st = g->ctx->stream;

@@ -161,6 +161,7 @@ _lib.bind(
         "hm_count_static": (C.c_int, [vp, u64p]),
         "hm_count_static30": (C.c_int, [vp, u64p]),
         "hm_count_static30_shard": (C.c_int, [vp, C.c_uint32, C.c_uint32, u64p]),
+        "hm_count_static30_async": (C.c_int, [vp, vp, vp]),
         "hm_graph_traffic": (C.c_int, [vp, C.POINTER(Traffic)]),
         "hm_graph_apply_batch": (C.c_int, [vp, u32p, C.c_uint32, u64p, u32p, C.c_uint32, u32p, i64p]),
         "hm_graph_live_ids": (C.c_int, [vp, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -292,6 +293,13 @@ class Graph:
         out = np.zeros(N_STATIC_CLASSES, np.uint64)
         check(lib.hm_count_static30_shard(self._h, shard, n_shards, ptr(out, C.c_uint64)), "hm_count_static30_shard")
         return out
+
+    def count_static30_async(self, d_out30: int, stream: int | None = None) -> None:
+        """Queues the 30-class count after the work on `stream` (a
+        cudaStream_t as an int; None: the context stream); the counts land in
+        the 30 uint64 at device address d_out30 without a host wait."""
+        check(lib.hm_count_static30_async(self._h, vp(d_out30), vp(stream) if stream else None),
+              "hm_count_static30_async")
 
     def traffic(self) -> Traffic:
         t = Traffic()

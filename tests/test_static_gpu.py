@@ -119,3 +119,27 @@ def test_static_shards_sum_to_full_count(ctx, n_shards):
         full = g.count_static30()
         parts = sum(g.count_static30_shard(s, n_shards) for s in range(n_shards))
     assert parts.tolist() == full.tolist()
+
+
+def test_async_count_on_caller_and_context_streams(ctx):
+    """hm_count_static30_async: queued after a caller's stream (twice in a
+    row, reusing the graph's counters) and on the context stream, the counts
+    reach the caller's device buffers and equal the oracle."""
+    import torch
+
+    from ipdps26_b200 import engine, gen
+
+    h = gen.static(gen.config1(seed=78, n_nodes=600, n_edges=1200))
+    want = oracle.static30(h.offsets, h.members, h.n_nodes)
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        s = torch.cuda.Stream(device=0)
+        outs = [torch.full((30,), -1, dtype=torch.int64, device="cuda:0") for _ in range(3)]
+        torch.cuda.synchronize()
+        g.count_static30_async(outs[0].data_ptr(), s.cuda_stream)
+        g.count_static30_async(outs[1].data_ptr(), s.cuda_stream)
+        s.synchronize()
+        g.count_static30_async(outs[2].data_ptr(), None)
+        torch.cuda.synchronize()
+        for o in outs:
+            assert o.cpu().numpy().view(np.uint64).tolist() == want.tolist()
+        assert g.count_static30().tolist() == want.tolist()
