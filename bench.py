@@ -49,37 +49,51 @@ def parse():
                     help="autotuner sample: every n-th centre (0: at most 65536 centres)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
-    ap.add_argument("--update-batches", type=int, default=20,
+    ap.add_argument("--cpu-sample-edges", type=int, default=40_000,
+                    help="the CPU baseline (and the reference arm) counts the first this many hyperedges of the "
+                         "workload; the GPU counts the same sample beside it")
+    ap.add_argument("--update-batches", type=int, default=100,
                     help="config-3 batches applied to the resident graph after the static steps (0: skip)")
-    ap.add_argument("--no-update-check", action="store_true",
-                    help="skip the full recount that checks the summed deltas")
+    ap.add_argument("--update-check-every", type=int, default=25,
+                    help="full recount checking the running delta sum after every this many batches and after "
+                         "the last (0: no check)")
     ap.add_argument("--no-temporal", action="store_true")
+    ap.add_argument("--no-temporal-cpu", action="store_true")
+    ap.add_argument("--temporal-samples", default="1000:50000,10000:10000,100000:1000",
+                    help="delta:events pairs: THyMe+ on the first `events` events of config 4 for each delta, "
+                         "the GPU on the same sample beside it")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-graphs", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="offered requests per second (Poisson)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the replayed trace")
+    ap.add_argument("--serve-low-rate", type=float, default=100.0,
+                    help="a second, sustainable offered rate, for latencies that are service times (0: skip)")
+    ap.add_argument("--serve-low-seconds", type=float, default=5.0)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     return ap.parse_args()
+
+
+def laws(args):
+    from ipdps26_b200 import workloads
+
+    return workloads.config2_laws(args.edges, args.nodes)
 
 
 def workload(args):
     from ipdps26_b200 import gen
 
-    q = gen.C2_Q * args.edges / 2_000_000
-    p = gen.config2(seed=1, n_nodes=args.nodes, n_edges=args.edges, q=q)
+    p = gen.from_laws(laws(args))
     return p, gen.static(p)
 
 
 def config_of(args, n_gpus):
-    from ipdps26_b200 import gen
-
+    L = laws(args)
     return {
         "workload": "config2-static-count",
         "hyperedges": args.edges,
         "nodes": args.nodes,
         "sizes": "k^-2.2 on [2,100]",
-        "popularity": f"Zipf-Mandelbrot s=1.1 q={gen.C2_Q * args.edges / 2_000_000:g}",
+        "popularity": f"Zipf-Mandelbrot s=1.1 q={L.q:g}",
         "seed": 1,
         "parallelism": f"centre-shard x{n_gpus} (replicated store)" if n_gpus > 1 else "single GPU",
         "l2": "inputs larger than L2 (store of tens of GB per step)",
@@ -156,36 +170,60 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(h, budget_s: float):
-    """The reference's own OpenMP counter (MoCHy main_exact_par, built from the
-    reference sources into oracle/_ref) on all host cores, on a bounded
-    sample: the first E' hyperedges of the same workload, E' doubled until
-    one run takes about budget_s."""
+def mochy_sample(args, path):
+    """Writes the first --cpu-sample-edges hyperedges of the workload in
+    MoCHy's format with hmgen (host code only; nothing of the engine is
+    loaded) and returns the number of hyperedges written."""
+    from ipdps26_b200 import workloads
+
+    n, _ = workloads.write_static(laws(args), path, prefix=min(args.cpu_sample_edges, args.edges))
+    return n
+
+
+def run_mochy_sample(path, cores):
+    """One timed run of the reference's own OpenMP counter (MoCHy
+    main_exact_par, built from the reference sources into oracle/_ref) on all
+    host cores: (26 counts, wall seconds including its file parse, its own
+    TOTAL_RUNTIME_SECONDS, which leaves the parse out)."""
     from oracle import ref_runner as rr
+
+    return rr.run_mochy_file(path, threads=cores, timeout=3600)
+
+
+def cpu_baseline(args, h, ctx):
+    """MoCHy main_exact_par on the first --cpu-sample-edges hyperedges of the
+    workload, timed on the host cores, and the GPU's static count of the very
+    same sample beside it: its device time, and whether its 26 counts equal
+    the ones MoCHy printed."""
+    import tempfile
+
+    from oracle import ref_runner as rr
+    from ipdps26_b200 import engine
 
     if not rr.available("mochy_exact_par"):
         return None
     cores = os.cpu_count() or 1
-    n = min(10_000, h.n_edges)
-    best = None
-    while n <= h.n_edges:
-        sub = h.subgraph(n)
-        try:
-            counts, wall, _ = rr.run_mochy(sub.offsets, sub.members, threads=cores, timeout=max(120, budget_s * 8))
-        except Exception as e:  # noqa: BLE001
-            if best is None:
-                return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
-                        "sample": f"failed at {n} hyperedges: {e}"}
-            break
-        best = (n, int(counts.sum()), wall)
-        if wall >= budget_s or n == h.n_edges:
-            break
-        n = min(h.n_edges, n * 2)
-    n, triples, wall = best
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "sample.txt")
+        n = mochy_sample(args, path)
+        counts, wall, self_s = run_mochy_sample(path, cores)
+    triples = int(counts.sum())
+    sub = h.subgraph(n)
+    with engine.Graph.from_hypergraph(ctx, sub) as g:
+        g.count_static()  # prepares the oriented rows and captures the launches
+        ms = []
+        for _ in range(5):
+            gpu26 = g.count_static()
+            ms.append(g.timings().count_ms)
+    gpu_s = statistics.median(ms) / 1000.0
     return {"value": triples / wall, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"MoCHy main_exact_par, first {n} hyperedges of the workload (same laws and node universe), "
-                      f"{triples} triples (26 motifs) in {wall:.2f} s wall including its file parse",
-            "wall_s": wall, "sample_hyperedges": n}
+            "sample": f"MoCHy main_exact_par on all {cores} host cores, first {n} hyperedges of the workload "
+                      f"(same laws and node universe), {triples} triples (26 motifs) in {wall:.2f} s wall "
+                      f"including its file parse ({self_s:.2f} s by its own clock, parse excluded)",
+            "sample_hyperedges": n, "wall_s": wall, "self_reported_s": self_s,
+            "gpu_same_sample_value": int(gpu26.sum()) / gpu_s, "gpu_same_sample_ms": 1000.0 * gpu_s,
+            "gpu_over_cpu_same_sample": (int(gpu26.sum()) / gpu_s) / (triples / wall),
+            "parity": bool(np.array_equal(gpu26, counts))}
 
 
 def pct(xs, q):
@@ -196,15 +234,17 @@ def pct(xs, q):
 
 def update_section(args, g, p, counts30):
     """Config 3: update batches on the resident config-2 graph, each with its
-    exact incremental recount; the summed deltas are checked against one full
-    recount at the end. Batch sizes are log-uniform in [1000, 100000] edits,
-    80 % insertions drawn from the config-2 laws, 20 % deletions uniform over
-    the live hyperedges (seed 2)."""
+    exact incremental recount (hm_graph_apply_batch with the delta). The
+    running sum of the deltas is checked against a full recount after every
+    --update-check-every batches and after the last one. Batch sizes are
+    log-uniform in [1000, 100000] edits, 80 % insertions drawn from the
+    config-2 laws, 20 % deletions uniform over the live hyperedges (seed 2)."""
     from ipdps26_b200 import gen
 
     rng = np.random.default_rng(2)
     total = counts30.astype(np.int64).copy()
-    wall, dev, sizes = [], [], []
+    wall, dev, sizes, checks = [], [], [], []
+    every = args.update_check_every
     for b in range(args.update_batches):
         n_edits = int(np.exp(rng.uniform(np.log(1_000), np.log(100_000))))
         live = g.live_ids()
@@ -215,31 +255,96 @@ def update_section(args, g, p, counts30):
         dev.append(g.timings().update_ms / 1000.0)
         sizes.append(n_edits)
         total += delta
+        if every and ((b + 1) % every == 0 or b + 1 == args.update_batches):
+            full = g.count_static30().astype(np.int64)
+            checks.append({"after_batch": b + 1, "equal": bool(np.array_equal(full, total))})
     out = {"batches": len(wall), "edits_min": min(sizes), "edits_max": max(sizes),
            "edits_total": int(sum(sizes)), "p50_ms": 1000 * pct(wall, 50), "p99_ms": 1000 * pct(wall, 99),
            "device_p50_ms": 1000 * pct(dev, 50), "device_p99_ms": 1000 * pct(dev, 99),
            "batches_per_s": len(wall) / sum(wall), "edits_per_s": sum(sizes) / sum(wall),
-           "form": "plain per-call (hm_graph_apply_batch with the exact delta)"}
-    if not args.no_update_check:
-        full = g.count_static30().astype(np.int64)
-        out["delta_sum_equals_full_recount"] = bool(np.array_equal(full, total))
+           "form": "plain per-call (hm_graph_apply_batch with the exact delta)",
+           "recount_checks": checks,
+           "delta_sum_equals_full_recount": bool(checks) and all(c["equal"] for c in checks)}
     return out
 
 
-def temporal_section(ctx):
+def temporal_samples(args):
+    out = []
+    for item in args.temporal_samples.split(","):
+        d, n = item.split(":")
+        out.append((int(d), int(n)))
+    return out
+
+
+def thyme_sample(delta, n_events, cores):
+    """THyMe+ (main_thymeP, built from the reference sources into
+    oracle/_ref) on the first n_events events of config 4, written in THyMe's
+    format by hmgen: (96 counts, wall seconds, its own clock() seconds summed
+    over threads)."""
+    import tempfile
+
+    from oracle import ref_runner as rr
+    from ipdps26_b200 import workloads as W
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "events.txt")
+        W.write_temporal(W.CONFIG4, W.CONFIG4_BURSTS, path, prefix=n_events)
+        return rr.run_thymeP_file(path, delta, cores, timeout=3600)
+
+
+def temporal_section(args, ctx):
     """Config 4: THyMe's 96 temporal motifs over 500K bursty events, for
-    delta in {1e3, 1e4, 1e5} (device time of one count each)."""
+    delta in {1e3, 1e4, 1e5}: device time of one count each, its algorithmic
+    bytes (the window-projection walk, hm_graph_temporal_traffic) as a
+    roofline, and the reference's own THyMe+ on all host cores on a prefix of
+    the same stream with the GPU on that prefix beside it (counts compared)."""
+    from oracle import ref_runner as rr
     from ipdps26_b200 import engine, gen
 
-    h = gen.temporal(gen.config4())
-    res = {"events": h.n_edges, "workload": "config4 seed=3 200K nodes, Zipf(1.2), bursty span 1e8"}
+    hbm, peak_kind = peaks()
+    h = gen.config4_temporal()
+    res = {"events": h.n_edges, "workload": "config4 seed=3 200K nodes, Zipf(1.2), bursty span 1e8",
+           "roofline_peak_gbs": hbm, "roofline_peak_kind": peak_kind}
+    samples = dict(temporal_samples(args))
+    cores = os.cpu_count() or 1
     with engine.Graph.from_hypergraph(ctx, h) as g:
         for d in (1_000, 10_000, 100_000):
             c = g.count_temporal(d)
-            c = g.count_temporal(d)
-            ms = g.timings().temporal_ms
-            res[f"delta_{d}"] = {"ms": ms, "instances_counted": int(c.sum()),
-                                 "temporal_triples_per_s": float(c.sum()) / (ms / 1000.0)}
+            ms = []
+            for _ in range(3):
+                c = g.count_temporal(d)
+                ms.append(g.timings().temporal_ms)
+            t_ms = statistics.median(ms)
+            tr = g.temporal_traffic()
+            achieved = tr.b_temp / (t_ms / 1000.0) / 1e9
+            res[f"delta_{d}"] = {
+                "ms": t_ms, "instances_counted": int(c.sum()),
+                "temporal_triples_per_s": float(c.sum()) / (t_ms / 1000.0),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "algorithmic_bytes": int(tr.b_temp),
+                             "window_neighbours": int(tr.window_neighbours), "closed_pairs": int(tr.closed_pairs),
+                             "open_pairs": int(tr.open_pairs), "kernel": "k_temporal (one block per event)"}}
+    if args.no_temporal_cpu or not rr.available("thymeP"):
+        return res
+    for d, n in temporal_samples(args):
+        ref, wall, cpu_s = thyme_sample(d, n, cores)
+        sub = h.subgraph(n)
+        with engine.Graph.from_hypergraph(ctx, sub) as gs:
+            got = gs.count_temporal(d)
+            ms = []
+            for _ in range(3):
+                got = gs.count_temporal(d)
+                ms.append(gs.timings().temporal_ms)
+        gpu_s = statistics.median(ms) / 1000.0
+        inst = int(ref.sum())
+        res.setdefault(f"delta_{d}", {})["cpu_baseline"] = {
+            "value": inst / wall, "unit": "instances/s", "cores": cores, "kind": "reference",
+            "sample": f"THyMe+ main_thymeP on all {cores} host cores, first {n} events of config 4, "
+                      f"{inst} instances in {wall:.2f} s wall ({cpu_s:.1f} s of CPU time by its own clock)",
+            "sample_events": n, "wall_s": wall, "self_reported_cpu_s": cpu_s,
+            "gpu_same_sample_value": float(got.sum()) / gpu_s, "gpu_same_sample_ms": 1000.0 * gpu_s,
+            "gpu_over_cpu_same_sample": (float(got.sum()) / gpu_s) / (inst / wall),
+            "parity": bool(np.array_equal(got, ref))}
     return res
 
 
@@ -247,14 +352,20 @@ def serve_section(args, ctx):
     """Config 5: resident graphs behind the request loop. One seeded trace of
     Poisson arrivals (70 % update batches of 100-10,000 edits, 80/20
     insert/delete, 30 % full counts) is replayed at its arrival times through
-    the per-request form (one store per graph, one call per request, every
-    count request a full count: the plain per-call form) and through the
-    batched form (pooled store, one round of launches serves the oldest
-    waiting request of every graph), once with counts kept current by the
-    exact deltas after a graph's first full count ("batched") and once
-    counting in full every time ("batched_recount"); every result of the
-    three replays must be identical. Latencies are submit-to-done on the
-    server clock."""
+    four forms:
+      per_request          one store per graph, one call per request, every
+                           count request a full count (the plain per-call form);
+      per_request_kept     the same, counts kept current by the exact deltas
+                           after a graph's first full count;
+      batched              pooled store, one round of launches serves the
+                           oldest waiting request of every graph, kept counts;
+      batched_recount      the same, counting in full every time.
+    Every result of the four replays must be identical. The batching speed-up
+    at equal count semantics is batched / per_request_kept and
+    batched_recount / per_request. At --serve-rate both forms are saturated,
+    so their latencies are queueing; a second trace at --serve-low-rate, which
+    both forms sustain, gives latencies that are service times. Latencies are
+    submit-to-done on the server clock."""
     from ipdps26_b200 import engine, gen, serve_trace
 
     ps = [gen.config5_graph(i) for i in range(args.serve_graphs)]
@@ -270,10 +381,8 @@ def serve_section(args, ctx):
         "edits": int(sum(r.edits for r in trace if r.kind == engine.REQ_UPDATE)),
         "trace_gen_s": time.perf_counter() - t0, "budget_gb": args.serve_budget_gb,
     }
-    reps = {}
-    forms = (("per_request", engine.SERVE_PER_REQUEST, False), ("batched", engine.SERVE_BATCHED, True),
-             ("batched_recount", engine.SERVE_BATCHED, False))
-    for name, mode, from_deltas in forms:
+
+    def run(name, mode, from_deltas, tr):
         with engine.Server(ctx, mode, mem_budget_bytes=int(args.serve_budget_gb * 1e9),
                            count_from_deltas=from_deltas) as srv:
             for h in hs:
@@ -281,50 +390,76 @@ def serve_section(args, ctx):
             t0 = time.perf_counter()
             srv.start()
             build_s = time.perf_counter() - t0
-            rep = serve_trace.replay(srv, trace)
+            rep = serve_trace.replay(srv, tr)
             st = srv.stats()
-        reps[name] = rep
-        out[name] = {**serve_trace.summarize(trace, rep), "build_s": build_s, "rounds": int(st.rounds),
+        return rep, {**serve_trace.summarize(tr, rep), "build_s": build_s, "rounds": int(st.rounds),
                      "device_gb_after": st.device_bytes / 1e9}
-    out["same_results"] = (serve_trace.same_results(reps["per_request"], reps["batched"])
-                           and serve_trace.same_results(reps["per_request"], reps["batched_recount"]))
-    out["update_throughput_ratio"] = (out["batched"]["update_batches_per_s"]
-                                      / out["per_request"]["update_batches_per_s"])
-    out["batching_only_ratio"] = (out["batched_recount"]["update_batches_per_s"]
-                                  / out["per_request"]["update_batches_per_s"])
+
+    forms = (("per_request", engine.SERVE_PER_REQUEST, False), ("per_request_kept", engine.SERVE_PER_REQUEST, True),
+             ("batched", engine.SERVE_BATCHED, True), ("batched_recount", engine.SERVE_BATCHED, False))
+    reps = {}
+    for name, mode, from_deltas in forms:
+        reps[name], out[name] = run(name, mode, from_deltas, trace)
+    base = reps["per_request"]
+    out["same_results"] = all(serve_trace.same_results(base, reps[k]) for k in reps if k != "per_request")
+    ups = {k: out[k]["update_batches_per_s"] for k, _, _ in forms}
+    out["update_throughput_ratio"] = ups["batched"] / ups["per_request"]
+    out["batching_ratio_kept_counts"] = ups["batched"] / ups["per_request_kept"]
+    out["batching_only_ratio"] = ups["batched_recount"] / ups["per_request"]
+    if args.serve_low_rate > 0:
+        low = serve_trace.make_trace(ps, rate=args.serve_low_rate, duration=args.serve_low_seconds, seed=6)
+        lo = {"offered_req_per_s": args.serve_low_rate, "seconds": args.serve_low_seconds, "requests": len(low)}
+        lreps = {}
+        for name, mode, from_deltas in (forms[1], forms[2]):
+            lreps[name], lo[name] = run(name, mode, from_deltas, low)
+        lo["same_results"] = serve_trace.same_results(lreps["per_request_kept"], lreps["batched"])
+        out["sustained"] = lo
     return out
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU counter (MoCHy main_exact_par on all host
+    cores, from oracle/_ref) on a bounded sample of the workload: its first
+    --cpu-sample-edges hyperedges, written by the host-only hmgen tool, so
+    that this process maps nothing of the engine. Each step is one run of the
+    program on that sample (wall time including its file parse). The sample is
+    stated in `config`: the reference cannot count the full 2M-hyperedge
+    workload in a bench run (days of CPU time at its measured rate)."""
     if rank != 0:
         return
-    p, h = workload(args)
-    base = cpu_baseline(h, args.cpu_sample_seconds)
-    cfg = config_of(args, 1)
-    if base is None or base.get("value") is None:
-        why = "reference counter (oracle/_ref) not built here" if base is None else base["sample"]
-        print(json.dumps({"impl": "reference", "unavailable": why}))
-        return
-    n = base["sample_hyperedges"]
-    sub = h.subgraph(n)
+    import tempfile
+
     from oracle import ref_runner as rr
 
-    cores = base["cores"]
-    for _ in range(args.warmup):
-        rr.run_mochy(sub.offsets, sub.members, threads=cores)
-    walls, triples = [], 0
-    for _ in range(args.steps):
-        c, w, _ = rr.run_mochy(sub.offsets, sub.members, threads=cores)
-        walls.append(w)
-        triples = int(c.sum())
+    if not rr.available("mochy_exact_par"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference counter (oracle/_ref) not built here"}))
+        return
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "sample.txt")
+        n = mochy_sample(args, path)
+        for _ in range(args.warmup):
+            run_mochy_sample(path, cores)
+        walls, selfs, triples = [], [], 0
+        for _ in range(args.steps):
+            c, w, s_self = run_mochy_sample(path, cores)
+            walls.append(w)
+            selfs.append(s_self)
+            triples = int(c.sum())
     t = sum(walls)
     value = triples * args.steps / t
+    cfg = {**config_of(args, 1), "parallelism": f"OpenMP, {cores} host threads",
+           "sample_hyperedges": n,
+           "sample": f"first {n} of the {args.edges} hyperedges (same laws and node universe)"}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": base["sample"]},
+                         "sample": f"MoCHy main_exact_par, first {n} hyperedges of the workload, {triples} triples "
+                                   f"(26 motifs) per run, {t / args.steps:.2f} s wall per run including its file "
+                                   f"parse ({statistics.mean(selfs):.2f} s by its own clock)",
+                         "sample_hyperedges": n},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -443,7 +578,7 @@ def engine_arm(args, rank, world, local_rank):
                    "note": "26 reported motifs; build of H2V/V2H/H2H included"}
         base = None
         if world == 1 and not args.no_cpu_baseline:
-            base = cpu_baseline(h, args.cpu_sample_seconds)
+            base = cpu_baseline(args, h, ctx)
         updates = None
         if args.update_batches > 0:
             updates = update_section(args, g, p, counts)
@@ -451,7 +586,7 @@ def engine_arm(args, rank, world, local_rank):
         g.close()  # the sections below build their own stores
         temporal = None
         if not args.no_temporal:
-            temporal = temporal_section(ctx)
+            temporal = temporal_section(args, ctx)
         serve = None
         if not args.no_serve:
             serve = serve_section(args, ctx)

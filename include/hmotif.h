@@ -195,6 +195,38 @@ int hm_graph_query(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t* offse
 int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32_t n_del, const uint64_t* ins_offsets,
                          const uint32_t* ins_members, uint32_t n_ins, uint32_t* assigned_ids_out,
                          int64_t* delta30_out);
+/* hm_graph_apply_batch ordered on a caller's stream: the batch's device work
+ * starts after the work already queued on `stream` (a cudaStream_t; NULL is
+ * the legacy default stream), and work queued on `stream` afterwards sees the
+ * updated store and, if d_delta30 (device memory, 30 int64) is not NULL, the
+ * exact delta there. The host returns once the batch is sequenced: a batch
+ * reads sizes back from the device between its steps, so the call does wait
+ * on the context stream, but never on the caller's. HM_ERR_STATE if `stream`
+ * is being captured into a CUDA graph. The reference's batch calls end in a
+ * device synchronize (dynamicHyperGraph/structure/operations.cu:82-356). */
+int hm_graph_apply_batch_async(hm_graph* g, const uint32_t* del_ids, uint32_t n_del, const uint64_t* ins_offsets,
+                               const uint32_t* ins_members, uint32_t n_ins, uint32_t* assigned_ids_out,
+                               int64_t* d_delta30, void* stream);
+
+/* Keyed fill: live hyperedge ids[i] gains the node ids
+ * values[prefix[i-1] .. prefix[i]) (prefix[-1] = 0; prefix holds the inclusive
+ * end of each id's values, the reference's insertPrefixSizes) and keeps its
+ * id. Members are a set: values it already holds are ignored. If delta30_out
+ * is not NULL it receives the exact change of the 30 static classes. Each id
+ * at most once per call; HM_ERR_NOT_LIVE if one is not live (nothing
+ * changes). Replaces fillCBST / CBSTOperations::insert(insertKeys,
+ * insertPayload, insertPrefixSizes) on H2V (dynamicHyperGraph/include/
+ * structure.hpp:38,54; structure/operations.cu:82-127, 417-419), with V2H
+ * and H2H kept in step. */
+int hm_graph_fill(hm_graph* g, const uint32_t* ids, uint32_t n, const uint32_t* values, const uint64_t* prefix,
+                  int64_t* delta30_out);
+/* Keyed unfill: the same with the values removed from each hyperedge's
+ * members (values it does not hold are ignored); a hyperedge left with no
+ * members stays live, with no neighbours. Replaces unfillCBST
+ * (dynamicHyperGraph/structure/operations.cu:439-453, kernel/unfill.cu:4-52). */
+int hm_graph_unfill(hm_graph* g, const uint32_t* ids, uint32_t n, const uint32_t* values, const uint64_t* prefix,
+                    int64_t* delta30_out);
+
 /* The ids of the live hyperedges in ascending order; *n_out receives their
  * number (out may be NULL to query it). */
 int hm_graph_live_ids(const hm_graph* g, uint32_t* out, uint32_t cap, uint32_t* n_out);
@@ -221,7 +253,9 @@ int hm_count_static30(hm_graph* g, uint64_t out30[HM_N_STATIC_CLASSES]);
  * allocator or fail for want of memory mid-request, code held to a fixed
  * memory reservation). No counterpart in the reference. d_ids (n ids) and
  * d_out30 (30 uint64) are device buffers owned by the caller; stream is a
- * cudaStream_t (NULL: the context stream). All scratch lives in one 8 MiB
+ * cudaStream_t, and NULL is CUDA's legacy default stream (torch's default
+ * stream): the kernels run on it after the work already queued there, and
+ * after any work the engine left on the context stream. All scratch lives in one 8 MiB
  * device array that the library sets aside when it is loaded: graphs of at
  * most 2^21 hyperedge slots, at most 2^20 distinct ids per call. The first
  * call on a device looks the array up and configures the kernels; make it
@@ -241,6 +275,17 @@ int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, uint32_t n, 
  * kernel, temporalDynamicHMotif/src/temporal_count.cu:91-217, bins 30 classes
  * of a different definition). */
 int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_MOTIFS]);
+/* The same, asynchronous: queued after the work already on `stream` (a
+ * cudaStream_t; NULL is the legacy default stream), the 96 counts land in
+ * d_out96 (device memory) and work queued on `stream` afterwards sees them;
+ * the call returns without waiting (the first count of a graph builds its
+ * time-ordered index first and waits for that). If an event has more than
+ * 2048 distinct neighbours inside its window, all 96 counts read 2^64 - 1
+ * (the synchronous call returns HM_ERR_LIMIT). HM_ERR_STATE if `stream` or
+ * the context stream is being captured into a CUDA graph. The reference's
+ * counters are host programs with no stream (THyMe-main/code/
+ * main_thymeP.cpp:117-388). */
+int hm_count_temporal_async(hm_graph* g, int64_t delta, uint64_t* d_out96, void* stream);
 
 /* Partial 30-class counts over one shard of the centres: the sum over
  * shard = 0 .. n_shards-1 equals hm_count_static30. One shard per GPU, each
@@ -249,13 +294,17 @@ int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_M
 int hm_count_static30_shard(hm_graph* g, uint32_t shard, uint32_t n_shards, uint64_t out30[HM_N_STATIC_CLASSES]);
 
 /* The 30-class static count, asynchronous: queued after the work already on
- * `stream` (a cudaStream_t; NULL: the context stream), it writes the counts
- * to d_out30 (device memory, 30 uint64) and returns without waiting; work
- * queued on `stream` afterwards sees them. The first call on a graph (and
- * the first after an update) prepares the oriented rows and the work list
- * and waits for that. Do not change the graph or count it again until the
- * stream has passed the count. The reference's calls all end in a device
- * synchronize (dynamicHyperGraph/src/HMotifCount.cu:97-125). */
+ * `stream` (a cudaStream_t; NULL is CUDA's legacy default stream, which is
+ * also torch's default stream; pass hm_ctx_stream(ctx) for the context
+ * stream), it writes the counts to d_out30 (device memory, 30 uint64) and
+ * returns without waiting; work queued on `stream` afterwards sees them. The
+ * first call on a graph (and the first after an update) prepares the
+ * oriented rows and the work list and waits for that. Do not change the graph
+ * or count it again until the stream has passed the count. HM_ERR_STATE if
+ * `stream` or the context stream is being captured into a CUDA graph. After
+ * this call hm_graph_timings reports the static phase times as -1 (not
+ * measured). The reference's calls all end in a device synchronize
+ * (dynamicHyperGraph/src/HMotifCount.cu:97-125). */
 int hm_count_static30_async(hm_graph* g, uint64_t* d_out30, void* stream);
 
 /* Algorithmic bytes of one static count of this graph (for rooflines):
@@ -337,6 +386,26 @@ typedef struct hm_timings_t {
   uint64_t closed_triangles;
 } hm_timings_t;
 int hm_graph_timings(const hm_graph* g, hm_timings_t* t);
+
+/* Algorithmic bytes of the last temporal count (for rooflines). For each
+ * event a, N(a) is the set of distinct hyperedges of its delta-window
+ * projection that share a node with it, d(a) = |N(a)|, and d_a(b) the degree
+ * of b in that projection. The bytes follow the reference algorithm's walk
+ * (THyMe-main/code/main_thymeP.cpp:219-334: the neighbours of a, then the
+ * neighbours of each of them), 8 bytes per adjacency entry:
+ *   b_temp = sum_a 8 d(a) + 8 sum_{b in N(a)} d_a(b),
+ * with sum_{b in N(a)} d_a(b) = d(a) + 2 closed_pairs(a) + open_pairs(a)
+ * (pairs of neighbours of a that overlap; pairs (b, c) with c adjacent to b
+ * but not to a). Zero before the first temporal count. */
+typedef struct hm_temporal_traffic_t {
+  uint64_t events;
+  int64_t delta;
+  uint64_t window_neighbours; /* sum_a d(a) */
+  uint64_t closed_pairs;      /* sum_a closed_pairs(a) */
+  uint64_t open_pairs;        /* sum_a open_pairs(a) */
+  uint64_t b_temp;
+} hm_temporal_traffic_t;
+int hm_graph_temporal_traffic(const hm_graph* g, hm_temporal_traffic_t* t);
 
 /* Class of a 7-bit region pattern: static class 0..29 or temporal motif
  * 0..95 (-1 if the pattern is not a connected triple). Bits: exclusive parts

@@ -99,6 +99,24 @@ class HypergraphStore {
     return update({}, payload, prefixSizes, delta30);
   }
 
+  // CBSTOperations::insert(insertKeys, insertPayload, insertPrefixSizes)
+  // (structure.hpp:54), i.e. fillCBST (structure/operations.cu:82-127,
+  // 417-419): the values are appended to the existing records insertKeys
+  // (1-based), insertPrefixSizes[i] the inclusive end of key i's values.
+  // Records keep their keys; values a record already holds are ignored (its
+  // members are a set). Optionally the exact 30-bin delta.
+  void insert(const std::vector<int>& insertKeys, const std::vector<int>& insertPayload,
+              const std::vector<int>& insertPrefixSizes, std::vector<int64_t>* delta30 = nullptr) {
+    edit_members(insertKeys, insertPayload, insertPrefixSizes, delta30, false);
+  }
+
+  // unfillCBST (structure/operations.cu:439-453): the values are removed from
+  // the records keysToUnfill.
+  void unfill(const std::vector<int>& keysToUnfill, const std::vector<int>& valuesToRemove,
+              const std::vector<int>& removePrefixSizes, std::vector<int64_t>* delta30 = nullptr) {
+    edit_members(keysToUnfill, valuesToRemove, removePrefixSizes, delta30, true);
+  }
+
   // deleteCBST (structure/operations.cu:129-175) on 1-based keys.
   void erase(const std::vector<int>& keys, std::vector<int64_t>* delta30 = nullptr) { update(keys, {}, {}, delta30); }
 
@@ -163,6 +181,22 @@ class HypergraphStore {
   hm_graph* context() const { return g_; }
 
  private:
+  void edit_members(const std::vector<int>& keys, const std::vector<int>& values, const std::vector<int>& prefix,
+                    std::vector<int64_t>* delta30, bool remove) {
+    if (keys.size() != prefix.size()) throw std::invalid_argument("insert/unfill: one prefix size per key");
+    std::vector<uint32_t> ids, vals;
+    for (int k : keys) ids.push_back((uint32_t)(k - 1));
+    for (int v : values) vals.push_back((uint32_t)v);
+    if (vals.empty()) vals.push_back(0);
+    std::vector<uint64_t> ends(prefix.begin(), prefix.end());
+    if (ends.empty()) ends.push_back(0);
+    std::vector<int64_t> d(HM_N_STATIC_CLASSES);
+    const int s = remove ? hm_graph_unfill(g_, ids.data(), (uint32_t)keys.size(), vals.data(), ends.data(), d.data())
+                         : hm_graph_fill(g_, ids.data(), (uint32_t)keys.size(), vals.data(), ends.data(), d.data());
+    check(s, remove ? "hm_graph_unfill" : "hm_graph_fill");
+    if (delta30) *delta30 = d;
+  }
+
   Context& ctx_;
   std::string name_;
   hm_graph* g_ = nullptr;

@@ -94,11 +94,33 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
     build_cli(force)
+    build_hmgen(force)
     return LIB
 
 
 CLI_SRC = PKG / "cli" / "hmotif_cli.cpp"
 CLI = PKG / "hmotif"
+HMGEN_SRCS = [PKG / "cli" / "hmgen.cpp", CSRC / "hm_gen.cpp", CSRC / "hm_io.cpp", CSRC / "hm_error.cpp"]
+HMGEN = PKG / "hmgen"
+
+
+def build_hmgen(force: bool = False) -> Path:
+    """The workload writer: the generator and file-format sources compiled
+    with g++ alone (no CUDA, no libhmotif.so), so that a process timing the
+    reference's own counters can produce the engine's exact inputs without
+    mapping the engine."""
+    deps = HMGEN_SRCS + [CSRC / "hm_internal.h", ROOT / "include" / "hmotif.h"]
+    if not force and not _stale(HMGEN, deps):
+        return HMGEN
+    cxx = shutil.which("g++") or "g++"
+    tmp = HMGEN.with_suffix(".tmp")
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", f"-I{CSRC}"] + [str(s) for s in HMGEN_SRCS] + \
+          ["-o", str(tmp)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed on hmgen:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, HMGEN)
+    return HMGEN
 
 
 def build_cli(force: bool = False) -> Path:

@@ -240,6 +240,50 @@ extern "C" int hm_graph_apply_batch(hm_graph* g, const uint32_t* del_ids, uint32
   return hm::apply_batch(g, del_ids, n_del, ins_offsets, ins_members, n_ins, assigned_ids_out, delta30_out);
 }
 
+extern "C" int hm_graph_fill(hm_graph* g, const uint32_t* ids, uint32_t n, const uint32_t* values,
+                             const uint64_t* prefix, int64_t* delta30_out) {
+  if (!g || (n && (!ids || !prefix || (prefix[n - 1] && !values))))
+    return hm::set_error(HM_ERR_INVALID, "hm_graph_fill: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::modify_members(g, ids, n, values, prefix, false, delta30_out);
+}
+
+extern "C" int hm_graph_unfill(hm_graph* g, const uint32_t* ids, uint32_t n, const uint32_t* values,
+                               const uint64_t* prefix, int64_t* delta30_out) {
+  if (!g || (n && (!ids || !prefix || (prefix[n - 1] && !values))))
+    return hm::set_error(HM_ERR_INVALID, "hm_graph_unfill: NULL argument");
+  CtxLock lock(g->ctx);
+  return hm::modify_members(g, ids, n, values, prefix, true, delta30_out);
+}
+
+namespace {
+struct Delta30 {
+  int64_t v[HM_N_STATIC_CLASSES];
+};
+__global__ void k_store_delta30(Delta30 d, int64_t* out) {
+  if (threadIdx.x < HM_N_STATIC_CLASSES) out[threadIdx.x] = d.v[threadIdx.x];
+}
+}  // namespace
+
+extern "C" int hm_graph_apply_batch_async(hm_graph* g, const uint32_t* del_ids, uint32_t n_del,
+                                          const uint64_t* ins_offsets, const uint32_t* ins_members, uint32_t n_ins,
+                                          uint32_t* assigned_ids_out, int64_t* d_delta30, void* stream) {
+  if (!g || (n_del && !del_ids) || (n_ins && (!ins_offsets || (ins_offsets[n_ins] && !ins_members))))
+    return hm::set_error(HM_ERR_INVALID, "hm_graph_apply_batch_async: NULL argument");
+  CtxLock lock(g->ctx);
+  const cudaStream_t user = static_cast<cudaStream_t>(stream);
+  hm::StreamOrder order(g->ctx->stream, user);
+  HM_TRY(order.begin("hm_graph_apply_batch_async"));
+  Delta30 d{};
+  HM_TRY(hm::apply_batch(g, del_ids, n_del, ins_offsets, ins_members, n_ins, assigned_ids_out,
+                         d_delta30 ? d.v : nullptr));
+  if (d_delta30) {
+    k_store_delta30<<<1, 32, 0, g->ctx->stream>>>(d, d_delta30);
+    HM_LAUNCH_CHECK();
+  }
+  return order.end("hm_graph_apply_batch_async");
+}
+
 extern "C" int hm_count_touching30(hm_graph* g, const uint32_t* ids, uint32_t n, uint64_t out30[HM_N_STATIC_CLASSES]) {
   if (!g || !out30 || (n && !ids)) return hm::set_error(HM_ERR_INVALID, "hm_count_touching30: NULL argument");
   HM_TRY(static_ok(g));
@@ -296,6 +340,27 @@ extern "C" int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N
   if (!g || !out96) return hm::set_error(HM_ERR_INVALID, "hm_count_temporal: NULL argument");
   CtxLock lock(g->ctx);
   return hm::count_temporal96(g, delta, out96);
+}
+
+extern "C" int hm_count_temporal_async(hm_graph* g, int64_t delta, uint64_t* d_out96, void* stream) {
+  if (!g || !d_out96) return hm::set_error(HM_ERR_INVALID, "hm_count_temporal_async: NULL argument");
+  CtxLock lock(g->ctx);
+  hm::StreamOrder order(g->ctx->stream, static_cast<cudaStream_t>(stream));
+  HM_TRY(order.begin("hm_count_temporal_async"));
+  HM_TRY(hm::count_temporal96_async(g, delta, d_out96));
+  return order.end("hm_count_temporal_async");
+}
+
+extern "C" int hm_graph_temporal_traffic(const hm_graph* g, hm_temporal_traffic_t* t) {
+  if (!g || !t) return hm::set_error(HM_ERR_INVALID, "hm_graph_temporal_traffic: NULL argument");
+  const hm::PhaseTimes& x = g->times;
+  t->events = x.t_events;
+  t->delta = x.t_delta;
+  t->window_neighbours = x.t_nbrs;
+  t->closed_pairs = x.t_closed_pairs;
+  t->open_pairs = x.t_open_pairs;
+  t->b_temp = 8 * x.t_nbrs + 8 * (x.t_nbrs + 2 * x.t_closed_pairs + x.t_open_pairs);
+  return HM_OK;
 }
 
 extern "C" int hm_debug_touch_orientation(hm_graph* g, int by_id) {

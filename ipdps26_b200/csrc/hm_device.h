@@ -86,6 +86,9 @@ struct DArr {
 struct PhaseTimes {
   float open_ms = 0, closed_ms = 0, total_ms = 0, update_ms = 0, temporal_ms = 0;
   uint64_t closed_triangles = 0;
+  // last temporal count: events, and the window-projection sizes it walked
+  uint64_t t_events = 0, t_nbrs = 0, t_closed_pairs = 0, t_open_pairs = 0;
+  int64_t t_delta = 0;
 };
 
 // Which launch shape of the closed phase takes a centre, by the length d of
@@ -234,6 +237,10 @@ int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P
 template <class T>
 int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n);
 
+// Temporal count (hm_temporal.cu): the 96 counts into device memory, queued
+// on the context stream (all 2^64 - 1 if an event's window overflows the table).
+int count_temporal96_async(hm_graph* g, int64_t delta, uint64_t* d_out96);
+
 // Static count (hm_static.cu).
 int prepare_static(hm_graph* g);
 int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_flags);
@@ -266,11 +273,56 @@ struct BatchHooks {
   std::function<int(const uint32_t* d_dels, uint32_t n_del)> before;  // old graph, deleted slots
   std::function<int(const uint32_t* d_ins, uint32_t n_ins)> after;    // new graph, assigned slots
 };
+// forced_ids (host, n_ins entries, or null): the ids the insertions take
+// instead of smallest-free-first; each must be free once the deletions ran.
 int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks);
+                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks,
+                      const uint32_t* forced_ids = nullptr);
 int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30);
+                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30,
+                const uint32_t* forced_ids = nullptr);
+// Members added to (remove = false) or removed from live hyperedges, ids kept.
+int modify_members(hm_graph* g, const uint32_t* h_ids, uint32_t n, const uint32_t* values, const uint64_t* prefix,
+                   bool remove, int64_t* delta30);
 int presize_h2h(hm_graph* g, uint32_t factor);
+
+// Orders the context stream's work after a caller's stream and the caller's
+// later work after it (two events); a null caller stream is CUDA's legacy
+// default stream. Refuses streams under CUDA-graph capture: the calls that use
+// it allocate from the context's pool and may wait on the context stream.
+struct StreamOrder {
+  cudaStream_t ctx_stream, user;
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  StreamOrder(cudaStream_t c, cudaStream_t u) : ctx_stream(c), user(u) {}
+  ~StreamOrder() {
+    for (auto x : e)
+      if (x) cudaEventDestroy(x);  // released once the recorded work completes
+  }
+  int begin(const char* where) {
+    for (cudaStream_t s : {user, ctx_stream}) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      const cudaError_t r = cudaStreamIsCapturing(s, &cs);
+      if (r != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return set_error(HM_ERR_STATE, "%s: the stream is being captured into a CUDA graph; call it outside the "
+                         "capture", where);
+      }
+    }
+    if (user == ctx_stream) return HM_OK;
+    HM_CUDA(cudaEventCreateWithFlags(&e[0], cudaEventDisableTiming));
+    HM_CUDA(cudaEventCreateWithFlags(&e[1], cudaEventDisableTiming));
+    HM_CUDA(cudaEventRecord(e[0], user));
+    HM_CUDA(cudaStreamWaitEvent(ctx_stream, e[0], 0));
+    return HM_OK;
+  }
+  int end(const char* where) {
+    (void)where;
+    if (user == ctx_stream) return HM_OK;
+    HM_CUDA(cudaEventRecord(e[1], ctx_stream));
+    HM_CUDA(cudaStreamWaitEvent(user, e[1], 0));
+    return HM_OK;
+  }
+};
 
 inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
   uint64_t b = (items + per_block - 1) / per_block;

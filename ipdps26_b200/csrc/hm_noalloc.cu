@@ -311,7 +311,12 @@ extern "C" int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, u
   HM_CUDA(cudaSetDevice(g->ctx->device));
   NaPtrs S;
   HM_TRY(na_setup(g->ctx->device, &S));
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->ctx->stream;
+  // NULL is CUDA's legacy default stream (torch's default stream too), so a
+  // caller's earlier work on it (the id upload, clearing d_out30) comes first.
+  // Work the engine queued on its own stream (an asynchronous static count)
+  // is finished before the kernels start.
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st != g->ctx->stream) HM_CUDA(cudaStreamSynchronize(g->ctx->stream));
   const uint32_t E = g->n_slots;
   const unsigned sms = (unsigned)g->ctx->n_sms;
   k_na_clear<<<sms * 4, kNaBlock, 0, st>>>(S, E);

@@ -766,13 +766,30 @@ __global__ void k_finish30(const unsigned long long* c, uint64_t* out30) {
 }
 }  // namespace
 
-// One count queued after `user` (the context stream when null), its classes
-// written to d_out30, no host wait once the graph is prepared.
+// One count queued after `user` (a null handle is CUDA's legacy default
+// stream, as everywhere in the runtime API), its classes written to d_out30,
+// no host wait once the graph is prepared. The launches run on the context
+// stream, ordered after `user` and before its later work by two events.
 int count_static30_async(hm_graph* g, uint64_t* d_out30, cudaStream_t user) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
+  // The first count of a graph captures its launches as CUDA graphs on the
+  // context stream and may wait on it; neither works inside a capture that
+  // the event below would pull the context stream into.
+  for (cudaStream_t s : {user, st}) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return set_error(HM_ERR_STATE, "async static count: the stream is being captured into a CUDA graph (%s); "
+                       "call it outside the capture", e != cudaSuccess ? cudaGetErrorString(e) : "active");
+    }
+  }
   HM_TRY(prepare_static(g));
-  const bool other = user && user != st;
+  // hm_graph_timings reports synchronous counts only; an asynchronous count
+  // is not waited for, so its phase times are marked as not measured.
+  g->times.open_ms = g->times.closed_ms = g->times.total_ms = -1.0f;
+  const bool other = user != st;
   cudaEvent_t e[2] = {nullptr, nullptr};
   auto release = [&]() {
     for (auto x : e)

@@ -180,6 +180,10 @@ struct TArgs {
   unsigned int* queue;
   unsigned long long* out;  // 96
   int* overflow;
+  // window-projection sizes behind the algorithmic bytes: [0] neighbours of
+  // each event in its window, [1] adjacent pairs among them, [2] pairs
+  // (b, c) with c adjacent to a neighbour b but not to the event
+  unsigned long long* stats;
 };
 
 // [first, last) of the sorted list x[0..n) restricted to values in [lo, hi)
@@ -243,6 +247,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
   __shared__ unsigned long long cnt96[96];
   __shared__ uint32_t s_item, s_nla;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  unsigned long long n_nbrs = 0, n_closed = 0, n_open_b = 0;  // this thread's share of A.stats
   for (unsigned k = threadIdx.x; k < 96; k += blockDim.x) cnt96[k] = 0;
   // the table is cleared once here; after each event only the slots it used
   // are reset (all of them after an overflow)
@@ -322,6 +327,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
       __syncthreads();
       continue;  // block-uniform; the whole count is reported as failed
     }
+    if (threadIdx.x == 0) n_nbrs += nla;
     const uint32_t* ao = A.opos + A.ooff[sa];
     uint32_t af, al;
     range_in(ao, A.olen[sa], lo, p, af, al);  // a's earlier occurrences in the window
@@ -345,6 +351,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
         uint32_t first;
         const uint32_t cbc = overlap(bm, bsz, cm, csz, first);
         uint32_t g = 0;
+        n_closed += cbc != 0;
         if (cbc) {
           if (asz <= 64) {
             g = __popcll(mb & mc);
@@ -427,6 +434,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
           uint32_t first;
           const uint32_t cbc = overlap(bm, bsz, cm, csz, first);
           if (first != v) continue;  // counted at the smallest shared node
+          ++n_open_b;
           const uint32_t* co = A.opos + A.ooff[c];
           uint32_t cf, cl;
           range_in(co, A.olen[c], lo, p, cf, cl);
@@ -448,6 +456,16 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
   __syncthreads();
   for (unsigned k = threadIdx.x; k < 96; k += blockDim.x)
     if (cnt96[k]) atomicAdd(&A.out[k], cnt96[k]);
+  for (int d = 16; d; d >>= 1) {
+    n_nbrs += __shfl_xor_sync(0xffffffffu, n_nbrs, d);
+    n_closed += __shfl_xor_sync(0xffffffffu, n_closed, d);
+    n_open_b += __shfl_xor_sync(0xffffffffu, n_open_b, d);
+  }
+  if (lane == 0) {
+    if (n_nbrs) atomicAdd(&A.stats[0], n_nbrs);
+    if (n_closed) atomicAdd(&A.stats[1], n_closed);
+    if (n_open_b) atomicAdd(&A.stats[2], n_open_b);
+  }
 }
 
 template <class K, class V>
@@ -558,29 +576,33 @@ static int build_temporal_index(hm_graph* g) {
   return HM_OK;
 }
 
-int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]) {
+namespace {
+// The 96 counts of one temporal count into the caller's buffer, or all ones
+// when an event's window overflowed the neighbour table.
+__global__ void k_temporal_finish(const unsigned long long* acc, uint64_t* out96) {
+  const unsigned k = threadIdx.x;
+  if (k < 96) out96[k] = acc[97] ? ~0ull : acc[k];
+}
+}  // namespace
+
+// Queues the window starts and the counting kernel on the context stream:
+// acc receives the 96 counts, [96] the work queue, [97] the overflow flag,
+// [98..100] the window-projection sizes. Events e0/e1 bracket the kernels.
+static int launch_temporal(hm_graph* g, int64_t delta, DArr<uint32_t>& lo, DArr<unsigned long long>& acc,
+                           cudaEvent_t e0, cudaEvent_t e1) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
-  for (int k = 0; k < 96; ++k) out96[k] = 0;
-  if (!g->temporal) return set_error(HM_ERR_STATE, "temporal count: the graph has no timestamps");
-  if (delta < 0) return set_error(HM_ERR_INVALID, "temporal count: delta must be >= 0");
   const uint32_t n = g->n_slots;
-  if (!n) return HM_OK;
   if (!g->t_ready) HM_TRY(build_temporal_index(g));
-  DArr<uint32_t> lo;
-  DArr<unsigned long long> acc;
   HM_TRY(lo.alloc(ctx, n));
-  HM_TRY(acc.alloc(ctx, 98));
-  HM_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 98, st));
-  cudaEvent_t e0, e1;
-  HM_CUDA(cudaEventCreate(&e0));
-  HM_CUDA(cudaEventCreate(&e1));
-  HM_CUDA(cudaEventRecord(e0, st));
+  HM_TRY(acc.alloc(ctx, 101));
+  HM_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 101, st));
+  if (e0) HM_CUDA(cudaEventRecord(e0, st));
   k_window_lo<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_time.p, n, delta, lo.p);
   HM_LAUNCH_CHECK();
   TArgs A{n, g->t_order.p, g->t_static.p, g->t_prev.p, lo.p, g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
           g->t_voff.p, g->t_vlen.p, g->t_vpos.p, g->t_ooff.p, g->t_olen.p, g->t_opos.p,
-          reinterpret_cast<unsigned int*>(acc.p + 96), acc.p, reinterpret_cast<int*>(acc.p + 97)};
+          reinterpret_cast<unsigned int*>(acc.p + 96), acc.p, reinterpret_cast<int*>(acc.p + 97), acc.p + 98};
   static bool attr = false;
   if (!attr) {
     HM_CUDA(cudaFuncSetAttribute(k_temporal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTemporalSmem));
@@ -588,20 +610,69 @@ int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]) {
   }
   k_temporal<<<std::min<unsigned>((unsigned)ctx->n_sms * 3, n), kBlock, kTemporalSmem, st>>>(A);
   HM_LAUNCH_CHECK();
-  HM_CUDA(cudaEventRecord(e1, st));
-  unsigned long long h[98];
-  HM_CUDA(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaStreamSynchronize(st));
+  if (e1) HM_CUDA(cudaEventRecord(e1, st));
+  return HM_OK;
+}
+
+static int temporal_args_ok(const hm_graph* g, int64_t delta) {
+  if (!g->temporal) return set_error(HM_ERR_STATE, "temporal count: the graph has no timestamps");
+  if (delta < 0) return set_error(HM_ERR_INVALID, "temporal count: delta must be >= 0");
+  return HM_OK;
+}
+
+int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < 96; ++k) out96[k] = 0;
+  HM_TRY(temporal_args_ok(g, delta));
+  const uint32_t n = g->n_slots;
+  if (!n) return HM_OK;
+  DArr<uint32_t> lo;
+  DArr<unsigned long long> acc;
+  cudaEvent_t e0, e1;
+  HM_CUDA(cudaEventCreate(&e0));
+  HM_CUDA(cudaEventCreate(&e1));
+  const int rc = launch_temporal(g, delta, lo, acc, e0, e1);
+  unsigned long long h[101];
+  cudaError_t ce = rc < 0 ? cudaSuccess : cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (rc >= 0 && ce == cudaSuccess) ce = cudaStreamSynchronize(st);
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
+  if (rc >= 0 && ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc < 0) return rc;
+  if (ce != cudaSuccess) return set_error(HM_ERR_CUDA, "temporal count: %s", cudaGetErrorString(ce));
   g->times.temporal_ms = ms;
+  g->times.t_events = n;
+  g->times.t_delta = delta;
+  g->times.t_nbrs = h[98];
+  g->times.t_closed_pairs = h[99];
+  g->times.t_open_pairs = h[100];
   if (h[97])
     return set_error(HM_ERR_LIMIT, "temporal count: an event has more than %u neighbours inside its window",
                      kMaxNbrs);
   for (int k = 0; k < 96; ++k) out96[k] = h[k];
   return HM_OK;
+}
+
+// The same, queued: no host wait once the time-ordered index exists; the
+// counts land in d_out96 (all ones on a window overflow). The timings and
+// the window-projection sizes of an asynchronous count are not read back.
+int count_temporal96_async(hm_graph* g, int64_t delta, uint64_t* d_out96) {
+  hm_ctx* ctx = g->ctx;
+  HM_TRY(temporal_args_ok(g, delta));
+  g->times.temporal_ms = -1.0f;
+  g->times.t_events = 0;
+  if (!g->n_slots) {
+    HM_CUDA(cudaMemsetAsync(d_out96, 0, sizeof(uint64_t) * 96, ctx->stream));
+    return HM_OK;
+  }
+  DArr<uint32_t> lo;
+  DArr<unsigned long long> acc;
+  HM_TRY(launch_temporal(g, delta, lo, acc, nullptr, nullptr));
+  k_temporal_finish<<<1, 96, 0, ctx->stream>>>(acc.p, d_out96);
+  HM_LAUNCH_CHECK();
+  return HM_OK;  // lo and acc are freed in stream order, after the kernels
 }
 
 }  // namespace hm

@@ -25,6 +25,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <iterator>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +62,14 @@ __global__ void k_check_live(const uint32_t* ids, uint32_t n, uint32_t n_slots, 
   for (uint64_t i = gtid(); i < n; i += gstride()) {
     const uint32_t id = ids[i];
     if (id >= n_slots || !is_live(bits, id)) atomicExch(bad, 1);
+  }
+}
+
+// Ids that must be free (not live) before they are given to insertions.
+__global__ void k_check_free(const uint32_t* ids, uint32_t n, uint32_t n_slots, const uint32_t* bits, int* bad) {
+  for (uint64_t i = gtid(); i < n; i += gstride()) {
+    const uint32_t id = ids[i];
+    if (id < n_slots && is_live(bits, id)) atomicExch(bad, 1);
   }
 }
 
@@ -615,7 +624,8 @@ struct PhaseTrace {
 // hooks.after the new graph and the assigned slots (both device arrays). All
 // device work; the host only sequences the kernels.
 int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks) {
+                      const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, const BatchHooks& hooks,
+                      const uint32_t* forced_ids) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   if (g->temporal) return set_error(HM_ERR_STATE, "apply_batch: temporal graphs are immutable");
@@ -624,6 +634,16 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
     std::sort(tmp.begin(), tmp.end());
     if (std::adjacent_find(tmp.begin(), tmp.end()) != tmp.end())
       return set_error(HM_ERR_INVALID, "apply_batch: a hyperedge id is deleted twice");
+  }
+  uint32_t forced_max = 0;
+  if (forced_ids && n_ins) {
+    std::vector<uint32_t> tmp(forced_ids, forced_ids + n_ins);
+    std::sort(tmp.begin(), tmp.end());
+    if (std::adjacent_find(tmp.begin(), tmp.end()) != tmp.end())
+      return set_error(HM_ERR_INVALID, "apply_batch: an id is given to two insertions");
+    forced_max = tmp.back();
+    if ((uint64_t)forced_max + 1 >= (1ull << 24))
+      return set_error(HM_ERR_LIMIT, "apply_batch: id %u beyond the 2^24 slot limit", forced_max);
   }
   if (n_ins) {
     if (h_ins_off[0] != 0) return set_error(HM_ERR_INVALID, "apply_batch: insert offsets must start at 0");
@@ -689,27 +709,45 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
     HM_LAUNCH_CHECK();
   }
 
-  // ---- assign ids: smallest free slots first, then new slots ---------------------
+  // ---- assign ids: smallest free slots first, then new slots (or the ids
+  // the caller gives, which must be free once the deletions are done) -----------
   const uint32_t words = (g->n_slots + 31) / 32;
   DArr<uint32_t> fcnt, ids;
   DArr<uint64_t> fpre;
-  HM_TRY(fcnt.alloc(ctx, words));
-  HM_TRY(fpre.alloc(ctx, (size_t)words + 1));
   HM_TRY(ids.alloc(ctx, n_ins));
-  if (words) {
-    k_free_counts<<<grid_for(words, kBlock), kBlock, 0, st>>>(g->live_bits.p, words, g->n_slots, fcnt.p);
-    HM_LAUNCH_CHECK();
+  uint32_t new_slots = g->n_slots;
+  if (forced_ids) {
+    if (n_ins) {
+      HM_CUDA(cudaMemcpyAsync(ids.p, forced_ids, sizeof(uint32_t) * n_ins, cudaMemcpyHostToDevice, st));
+      HM_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+      k_check_free<<<grid_for(n_ins, kBlock), kBlock, 0, st>>>(ids.p, n_ins, g->n_slots, g->live_bits.p, bad.p);
+      HM_LAUNCH_CHECK();
+      HM_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      HM_CUDA(cudaStreamSynchronize(st));
+      // the deletions already ran: the store is changed, so this is a caller
+      // error the entry points rule out before calling (ids they give are the
+      // ones they delete)
+      if (hbad) return set_error(HM_ERR_INVALID, "apply_batch: an insertion's id is in use");
+      new_slots = std::max(new_slots, forced_max + 1);
+    }
+  } else {
+    HM_TRY(fcnt.alloc(ctx, words));
+    HM_TRY(fpre.alloc(ctx, (size_t)words + 1));
+    if (words) {
+      k_free_counts<<<grid_for(words, kBlock), kBlock, 0, st>>>(g->live_bits.p, words, g->n_slots, fcnt.p);
+      HM_LAUNCH_CHECK();
+    }
+    HM_TRY(exclusive_scan(ctx, fcnt.p, fpre.p, words));
+    uint64_t n_free = 0;
+    HM_CUDA(cudaMemcpyAsync(&n_free, fpre.p + words, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    if (n_ins) {
+      k_assign<<<grid_for(n_ins, kBlock), kBlock, 0, st>>>(n_ins, n_free, fpre.p, g->live_bits.p, words, g->n_slots,
+                                                            ids.p);
+      HM_LAUNCH_CHECK();
+    }
+    new_slots = g->n_slots + (n_ins > n_free ? (uint32_t)(n_ins - n_free) : 0u);
   }
-  HM_TRY(exclusive_scan(ctx, fcnt.p, fpre.p, words));
-  uint64_t n_free = 0;
-  HM_CUDA(cudaMemcpyAsync(&n_free, fpre.p + words, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaStreamSynchronize(st));
-  if (n_ins) {
-    k_assign<<<grid_for(n_ins, kBlock), kBlock, 0, st>>>(n_ins, n_free, fpre.p, g->live_bits.p, words, g->n_slots,
-                                                          ids.p);
-    HM_LAUNCH_CHECK();
-  }
-  const uint32_t new_slots = g->n_slots + (n_ins > n_free ? (uint32_t)(n_ins - n_free) : 0u);
   if ((uint64_t)new_slots >= (1ull << 24))
     return set_error(HM_ERR_LIMIT, "apply_batch: %u hyperedge slots exceed the 2^24 limit", new_slots);
   HM_TRY(ensure_slots(g, new_slots));
@@ -956,15 +994,88 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
 // Exact change of the 30 static classes: touched triples of the inserted
 // hyperedges in the new graph minus those of the deleted ones in the old.
 int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint64_t* h_ins_off,
-                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30) {
-  if (!delta30) return apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, BatchHooks{});
+                const uint32_t* h_ins_mem, uint32_t n_ins, uint32_t* assigned_out, int64_t* delta30,
+                const uint32_t* forced_ids) {
+  if (!delta30)
+    return apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, BatchHooks{}, forced_ids);
   uint64_t before[30] = {0}, after[30] = {0};
   BatchHooks hooks;
   hooks.before = [&](const uint32_t* d, uint32_t n) { return n ? count_touching(g, d, n, before) : (int)HM_OK; };
   hooks.after = [&](const uint32_t* d, uint32_t n) { return n ? count_touching(g, d, n, after) : (int)HM_OK; };
-  HM_TRY(apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, hooks));
+  HM_TRY(apply_batch_hooks(g, h_dels, n_del, h_ins_off, h_ins_mem, n_ins, assigned_out, hooks, forced_ids));
   for (int k = 0; k < 30; ++k) delta30[k] = (int64_t)(after[k] - before[k]);
   return HM_OK;
+}
+
+// fillCBST / unfillCBST on H2V: the members of live hyperedges ids[0..n)
+// gain (or lose) the values [prefix[i-1], prefix[i]); each hyperedge keeps its
+// id. Done as one batch that deletes the hyperedges and inserts their new
+// member lists at the same ids, so the store, the adjacency and the exact
+// delta follow from the batch path.
+int modify_members(hm_graph* g, const uint32_t* h_ids, uint32_t n, const uint32_t* values, const uint64_t* prefix,
+                   bool remove, int64_t* delta30) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  if (g->temporal) return set_error(HM_ERR_STATE, "fill/unfill: temporal graphs are immutable");
+  if (!n) {
+    if (delta30)
+      for (int k = 0; k < 30; ++k) delta30[k] = 0;
+    return HM_OK;
+  }
+  for (uint32_t i = 0; i < n; ++i)
+    if (i && prefix[i] < prefix[i - 1]) return set_error(HM_ERR_INVALID, "fill/unfill: prefix sizes decrease");
+  {
+    std::vector<uint32_t> tmp(h_ids, h_ids + n);
+    std::sort(tmp.begin(), tmp.end());
+    if (std::adjacent_find(tmp.begin(), tmp.end()) != tmp.end())
+      return set_error(HM_ERR_INVALID, "fill/unfill: a hyperedge id is listed twice");
+  }
+  for (uint32_t i = 0; i < prefix[n - 1]; ++i)
+    if (values[i] >= g->n_nodes)
+      return set_error(HM_ERR_INVALID, "fill/unfill: node %u out of range (%u nodes)", values[i], g->n_nodes);
+  // current member lists (device -> host), the live check included
+  DArr<uint32_t> ids;
+  DArr<int> bad;
+  HM_TRY(ids.alloc(ctx, n));
+  HM_TRY(bad.alloc(ctx, 1));
+  HM_CUDA(cudaMemcpyAsync(ids.p, h_ids, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+  HM_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+  k_check_live<<<grid_for(n, kBlock), kBlock, 0, st>>>(ids.p, n, g->n_slots, g->live_bits.p, bad.p);
+  HM_LAUNCH_CHECK();
+  int hbad = 0;
+  HM_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  if (hbad) return set_error(HM_ERR_NOT_LIVE, "fill/unfill: a hyperedge id is not live");
+  std::vector<uint64_t> off(g->n_slots), cur_off(n + 1, 0);
+  std::vector<uint32_t> len(g->n_slots);
+  HM_CUDA(cudaMemcpyAsync(off.data(), g->h2v_off.p, sizeof(uint64_t) * g->n_slots, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaMemcpyAsync(len.data(), g->h2v_len.p, sizeof(uint32_t) * g->n_slots, cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  std::vector<uint64_t> new_off(n + 1, 0);
+  std::vector<uint32_t> new_mem, row;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t id = h_ids[i];
+    row.resize(len[id]);
+    if (len[id])
+      HM_CUDA(cudaMemcpyAsync(row.data(), g->h2v_mem.p + off[id], sizeof(uint32_t) * len[id], cudaMemcpyDeviceToHost,
+                              st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> vals(values + (i ? prefix[i - 1] : 0), values + prefix[i]);
+    std::sort(vals.begin(), vals.end());
+    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    std::vector<uint32_t> next;
+    if (remove)
+      std::set_difference(row.begin(), row.end(), vals.begin(), vals.end(), std::back_inserter(next));
+    else
+      std::set_union(row.begin(), row.end(), vals.begin(), vals.end(), std::back_inserter(next));
+    if (next.size() > HM_MAX_EDGE_SIZE)
+      return set_error(HM_ERR_LIMIT, "fill: hyperedge %u would have %zu members (limit %d)", id, next.size(),
+                       HM_MAX_EDGE_SIZE);
+    new_mem.insert(new_mem.end(), next.begin(), next.end());
+    new_off[i + 1] = new_mem.size();
+  }
+  if (new_mem.empty()) new_mem.push_back(0);  // a valid pointer for an all-empty batch
+  return apply_batch(g, h_ids, n, new_off.data(), new_mem.data(), n, nullptr, delta30, h_ids);
 }
 
 }  // namespace hm

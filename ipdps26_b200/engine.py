@@ -57,6 +57,17 @@ class Timings(C.Structure):
     ]
 
 
+class TemporalTraffic(C.Structure):
+    _fields_ = [
+        ("events", C.c_uint64),
+        ("delta", C.c_int64),
+        ("window_neighbours", C.c_uint64),
+        ("closed_pairs", C.c_uint64),
+        ("open_pairs", C.c_uint64),
+        ("b_temp", C.c_uint64),
+    ]
+
+
 class Schedule(C.Structure):
     """Launch splits of the static and touched-triple counts (hm_schedule)."""
 
@@ -167,6 +178,11 @@ _lib.bind(
         "hm_graph_live_ids": (C.c_int, [vp, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
         "hm_count_touching30": (C.c_int, [vp, u32p, C.c_uint32, u64p]),
         "hm_count_temporal": (C.c_int, [vp, C.c_int64, u64p]),
+        "hm_graph_temporal_traffic": (C.c_int, [vp, C.POINTER(TemporalTraffic)]),
+        "hm_count_temporal_async": (C.c_int, [vp, C.c_int64, vp, vp]),
+        "hm_graph_apply_batch_async": (C.c_int, [vp, u32p, C.c_uint32, u64p, u32p, C.c_uint32, u32p, vp, vp]),
+        "hm_graph_fill": (C.c_int, [vp, u32p, C.c_uint32, u32p, u64p, i64p]),
+        "hm_graph_unfill": (C.c_int, [vp, u32p, C.c_uint32, u32p, u64p, i64p]),
         "hm_debug_touch_orientation": (C.c_int, [vp, C.c_int]),
         "hm_count_vertex_triads": (C.c_int, [vp, u64p]),
         "hm_graph_set_schedule": (C.c_int, [vp, C.POINTER(Schedule)]),
@@ -296,10 +312,11 @@ class Graph:
 
     def count_static30_async(self, d_out30: int, stream: int | None = None) -> None:
         """Queues the 30-class count after the work on `stream` (a
-        cudaStream_t as an int; None: the context stream); the counts land in
-        the 30 uint64 at device address d_out30 without a host wait."""
-        check(lib.hm_count_static30_async(self._h, vp(d_out30), vp(stream) if stream else None),
-              "hm_count_static30_async")
+        cudaStream_t as an int, 0 being the legacy default stream that torch's
+        default stream is; None: the context stream); the counts land in the
+        30 uint64 at device address d_out30 without a host wait."""
+        s = lib.hm_ctx_stream(self.ctx.handle) if stream is None else stream
+        check(lib.hm_count_static30_async(self._h, vp(d_out30), vp(s)), "hm_count_static30_async")
 
     def traffic(self) -> Traffic:
         t = Traffic()
@@ -320,6 +337,45 @@ class Graph:
                                        ptr(ids, C.c_uint32), ptr(dl, C.c_int64)), "hm_graph_apply_batch")
         return ids[:n_ins].copy(), dl
 
+    def apply_batch_async(self, del_ids, ins_offsets=None, ins_members=None, d_delta30: int | None = None,
+                          stream: int | None = None) -> np.ndarray:
+        """hm_graph_apply_batch ordered on `stream` (a cudaStream_t as an int,
+        0 the legacy default stream; None the context stream); the delta, if
+        d_delta30 is a device address, lands there. Returns the assigned ids."""
+        d = np.ascontiguousarray(del_ids if del_ids is not None else [], dtype=np.uint32)
+        if ins_offsets is None:
+            ins_offsets, ins_members = np.zeros(1, np.uint64), np.zeros(0, np.uint32)
+        off, mem = _csr_arrays(ins_offsets, ins_members)
+        n_ins = len(off) - 1
+        ids = np.zeros(max(n_ins, 1), np.uint32)
+        s = lib.hm_ctx_stream(self.ctx.handle) if stream is None else stream
+        check(lib.hm_graph_apply_batch_async(self._h, ptr(d, C.c_uint32), len(d), ptr(off, C.c_uint64),
+                                             ptr(mem if len(mem) else np.zeros(1, np.uint32), C.c_uint32), n_ins,
+                                             ptr(ids, C.c_uint32), vp(d_delta30) if d_delta30 else None, vp(s)),
+              "hm_graph_apply_batch_async")
+        return ids[:n_ins].copy()
+
+    def _members_edit(self, fn, name, ids, values_per_id):
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        vals = [np.asarray(v, dtype=np.uint32) for v in values_per_id]
+        if len(vals) != len(ids):
+            raise ValueError(f"{name}: one value list per id")
+        prefix = np.cumsum([len(v) for v in vals]).astype(np.uint64) if len(vals) else np.zeros(0, np.uint64)
+        flat = np.concatenate(vals) if vals and sum(map(len, vals)) else np.zeros(1, np.uint32)
+        dl = np.zeros(N_STATIC_CLASSES, np.int64)
+        check(fn(self._h, ptr(ids, C.c_uint32), len(ids), ptr(flat, C.c_uint32),
+                 ptr(prefix if len(prefix) else np.zeros(1, np.uint64), C.c_uint64), ptr(dl, C.c_int64)), name)
+        return dl
+
+    def fill(self, ids, values_per_id) -> np.ndarray:
+        """Keyed fill (fillCBST): adds values_per_id[i] to the members of live
+        hyperedge ids[i], ids kept; returns the exact 30-class delta."""
+        return self._members_edit(lib.hm_graph_fill, "hm_graph_fill", ids, values_per_id)
+
+    def unfill(self, ids, values_per_id) -> np.ndarray:
+        """Keyed unfill (unfillCBST): removes the values from the members."""
+        return self._members_edit(lib.hm_graph_unfill, "hm_graph_unfill", ids, values_per_id)
+
     def live_ids(self) -> np.ndarray:
         n = C.c_uint32()
         check(lib.hm_graph_live_ids(self._h, None, 0, C.byref(n)), "hm_graph_live_ids")
@@ -331,6 +387,18 @@ class Graph:
         out = np.zeros(N_TEMPORAL_MOTIFS, np.uint64)
         check(lib.hm_count_temporal(self._h, int(delta), ptr(out, C.c_uint64)), "hm_count_temporal")
         return out
+
+    def count_temporal_async(self, delta: int, d_out96: int, stream: int | None = None) -> None:
+        """Queues the 96-motif count after the work on `stream` (0: the legacy
+        default stream; None: the context stream) into device memory d_out96."""
+        s = lib.hm_ctx_stream(self.ctx.handle) if stream is None else stream
+        check(lib.hm_count_temporal_async(self._h, int(delta), vp(d_out96), vp(s)), "hm_count_temporal_async")
+
+    def temporal_traffic(self) -> TemporalTraffic:
+        """Window-projection sizes and algorithmic bytes of the last temporal count."""
+        t = TemporalTraffic()
+        check(lib.hm_graph_temporal_traffic(self._h, C.byref(t)), "hm_graph_temporal_traffic")
+        return t
 
     def count_touching30(self, ids) -> np.ndarray:
         ids = np.ascontiguousarray(ids, dtype=np.uint32)

@@ -12,6 +12,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import workloads as W
 from ._lib import BurstParams, GenParams, HostGraphInfo, check, lib, ptr, vp
 
 
@@ -84,27 +85,33 @@ def batch(p: GenParams, batch_seed: int, live_ids: np.ndarray, n_edits: int, ins
     return dels[: nd.value].copy(), _take(h)
 
 
-# ---- named workloads -------------------------------------------------------
-# Config 1: 10K nodes, 20K hyperedges, sizes k^-2.5 on [2,25], Zipf(1.2).
+# ---- named workloads (parameters in workloads.py) ---------------------------
+C2_Q = W.C2_Q
+C5_Q = W.C5_Q
+
+
+def from_laws(L: W.Laws) -> GenParams:
+    return params(L.seed, L.n_nodes, L.n_edges, L.k_min, L.k_max, L.size_exp, L.pop_exp, L.q, dedupe=L.dedupe)
+
+
 def config1(seed: int = 0, n_nodes: int = 10_000, n_edges: int = 20_000, q: float = 0.0) -> GenParams:
-    return params(seed, n_nodes, n_edges, 2, 25, 2.5, 1.2, q)
-
-
-# Config 2: 1M nodes, 2M hyperedges, sizes k^-2.2 on [2,100], Zipf-Mandelbrot
-# s = 1.1 with offset q = 1000 (plain Zipf(1.1) makes the projection of this
-# size exceed device memory and any exact counter: a hub of degree ~770K and
-# about 1.1e17 triples sharing one node).
-C2_Q = 1000.0
+    return from_laws(W.CONFIG1.scaled(seed=seed, n_nodes=n_nodes, n_edges=n_edges, q=q))
 
 
 def config2(seed: int = 1, n_nodes: int = 1_000_000, n_edges: int = 2_000_000, q: float = C2_Q) -> GenParams:
-    return params(seed, n_nodes, n_edges, 2, 100, 2.2, 1.1, q)
+    return from_laws(W.CONFIG2.scaled(seed=seed, n_nodes=n_nodes, n_edges=n_edges, q=q))
 
 
-# Config 4: 500K timestamped hyperedges over 200K nodes, sizes k^-2.5 on
-# [2,20], Zipf(1.2); repeated node-sets are kept (they make motifs 87-96).
 def config4(seed: int = 3, n_nodes: int = 200_000, n_edges: int = 500_000, q: float = 0.0) -> GenParams:
-    return params(seed, n_nodes, n_edges, 2, 20, 2.5, 1.2, q, dedupe=False)
+    return from_laws(W.CONFIG4.scaled(seed=seed, n_nodes=n_nodes, n_edges=n_edges, q=q))
+
+
+def config4_temporal(n_edges: int = W.CONFIG4.n_edges) -> Hypergraph:
+    """Config 4's event stream (its first n_edges events when smaller: the
+    times of a prefix are those of the full stream)."""
+    B = W.CONFIG4_BURSTS
+    h = temporal(config4(), B.burst_rate, B.events_per_burst, B.gap_mean, B.span)
+    return h if n_edges >= h.n_edges else h.subgraph(n_edges)
 
 
 # Config 5: resident graphs with |E| log-uniform in [1e3, 2e5] (seeds 100 +
@@ -112,12 +119,8 @@ def config4(seed: int = 3, n_nodes: int = 200_000, n_edges: int = 500_000, q: fl
 # popularity with the Zipf-Mandelbrot offset q = 1000 of config 2 (with q = 0
 # a 200K-edge graph has a hub in about half of its hyperedges and ~1.8e14
 # triples sharing one node, hours of exact counting per request).
-C5_Q = 1000.0
-
-
 def config5_graph(i: int, e_min: int = 1000, e_max: int = 200_000, q: float = C5_Q) -> GenParams:
     seed = 100 + i
     u = np.random.default_rng(seed).uniform(np.log(e_min), np.log(e_max))
     n_edges = int(round(np.exp(u)))
     return params(seed, max(n_edges // 2, 2), n_edges, 2, 25, 2.5, 1.2, q)
-

@@ -32,4 +32,14 @@ if [ -d "$TD/src" ]; then
       "$TD/utils/utils.cpp" "$TD/utils/printUtils.cpp" "$TD/utils/flatten.cpp"
   done
 fi
+# The reference's own datasets with known outputs, copied verbatim for the
+# parity tests (refdata.py): MoCHy's dblp sample and THyMe's email-Enron with
+# its shipped results at delta = 86,400,000.
+mkdir -p "$OUT/data"
+for f in MoCHy-master/dblp_graph.txt THyMe-main/data/email-Enron-full/email-Enron-full.txt \
+    THyMe-main/results/email-Enron-full_86400000.000000_thyme.txt \
+    THyMe-main/results/email-Enron-full_86400000.000000_thymeP.txt \
+    THyMe-main/results/email-Enron-full_86400000.000000_dp.txt; do
+  if [ -f "$REF/$f" ]; then cp "$REF/$f" "$OUT/data/"; fi
+done
 echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"

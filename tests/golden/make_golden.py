@@ -27,9 +27,9 @@ sys.path.insert(0, str(ROOT))
 
 from ipdps26_b200 import gen  # noqa: E402
 from oracle import ref_runner as rr  # noqa: E402
+from oracle import refdata  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
-REF_DBLP = Path("/root/reference/MoCHy-master/dblp_graph.txt")
 
 
 def digest(h) -> str:
@@ -134,24 +134,31 @@ def main() -> None:
     tg = json.loads(tp.read_text()) if tp.exists() else {}
     want = set(a.only) if a.only else None
 
-    if REF_DBLP.exists() and (want is None or "dblp" in want):
-        lines = REF_DBLP.read_text().splitlines()
-        off, mem = [0], []
-        for ln in lines:
-            row = []
-            for t in ln.split(","):
-                v = int(t)
-                if v not in row:
-                    row.append(v)
-            mem += row
-            off.append(len(mem))
-        off, mem = np.array(off, np.uint64), np.array(mem, np.uint32)
+    dblp = refdata.path("dblp")
+    if dblp is not None and (want is None or "dblp" in want):
+        off, mem, _ = refdata.read_mochy(dblp)
         c, w, _ = rr.run_mochy(off, mem, threads=None, timeout=a.timeout)
         cp, wp, _ = rr.run_mochy(off, mem, threads=8, timeout=a.timeout)
         assert np.array_equal(c, cp)
-        sg["dblp"] = dict(file_sha256=hashlib.sha256(REF_DBLP.read_bytes()).hexdigest(), counts26=c.tolist(),
-                          n_edges=len(off) - 1, source="MoCHy-master/dblp_graph.txt", mochy_wall_s=round(w, 3))
+        sg["dblp"] = dict(file_sha256=hashlib.sha256(dblp.read_bytes()).hexdigest(), counts26=c.tolist(),
+                          n_edges=len(off) - 1, source=refdata.FILES["dblp"], mochy_wall_s=round(w, 3))
         print("dblp", w)
+
+    enron = refdata.path("email-Enron")
+    if enron is not None and (want is None or "email-Enron" in want):
+        # THyMe's shipped results for this dataset (three exact programs); the
+        # data has ties in time, so only tie-independent sums are recorded:
+        # the total and the sum per static class of the 96 motifs
+        res = {}
+        for k in ("thyme", "thymeP", "dp"):
+            rp = refdata.path(f"email-Enron-{k}")
+            _, c96 = refdata.read_thyme_result(rp)
+            res[k] = (int(c96.sum()), refdata.per_static(c96))
+        assert res["thyme"] == res["thymeP"] == res["dp"], "shipped results disagree"
+        tg["email-Enron"] = dict(file_sha256=refdata.sha256(enron), source=refdata.FILES["email-Enron"],
+                                 delta=refdata.ENRON_DELTA, total=res["thymeP"][0], per_static=res["thymeP"][1],
+                                 results=[refdata.FILES[f"email-Enron-{k}"] for k in ("thyme", "thymeP", "dp")])
+        print("email-Enron", res["thymeP"][0])
 
     for name, p in STATIC_CASES.items():
         if want is not None and name not in want:

@@ -6,29 +6,22 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from oracle import oracle
+from oracle import oracle, refdata
 from tests.helpers import csr, digest, load_golden, random_graph, static_case, temporal_case
 
-REF_DBLP = Path("/root/reference/MoCHy-master/dblp_graph.txt")
 ROOT = Path(__file__).resolve().parents[1]
+SYNTHETIC_TEMPORAL = sorted(k for k, v in load_golden("temporal").items() if "params" in v)
 
 
 @pytest.mark.parametrize("name", sorted(load_golden("static")))
 def test_static_oracle_matches_mochy(name):
     rec = load_golden("static")[name]
     if name == "dblp":
-        if not REF_DBLP.exists():
-            pytest.skip("reference dataset not present")
-        assert hashlib.sha256(REF_DBLP.read_bytes()).hexdigest() == rec["file_sha256"]
-        rows = []
-        for ln in REF_DBLP.read_text().splitlines():
-            r = []
-            for t in ln.split(","):
-                if int(t) not in r:
-                    r.append(int(t))
-            rows.append(r)
-        off, mem = csr(rows)
-        n_nodes = int(mem.max()) + 1
+        p = refdata.path("dblp")
+        if p is None:
+            pytest.skip("reference dataset not present (oracle/build_ref.sh copies it)")
+        assert hashlib.sha256(p.read_bytes()).hexdigest() == rec["file_sha256"]
+        off, mem, n_nodes = refdata.read_mochy(p)
     else:
         if rec["n_edges"] > 3000:
             pytest.skip("large case: covered by the GPU parity test")
@@ -39,7 +32,7 @@ def test_static_oracle_matches_mochy(name):
     assert got.tolist() == rec["counts26"]
 
 
-@pytest.mark.parametrize("name", sorted(load_golden("temporal")))
+@pytest.mark.parametrize("name", SYNTHETIC_TEMPORAL)
 def test_temporal_oracle_matches_thyme(name):
     rec = load_golden("temporal")[name]
     if rec["n_events"] > 2000:
@@ -49,6 +42,26 @@ def test_temporal_oracle_matches_thyme(name):
     for d, want in rec["counts96"].items():
         got = oracle.temporal96(h.offsets, h.members, h.timestamps, int(d))
         assert got.tolist() == want, d
+
+
+def test_temporal_oracle_on_thyme_email_enron():
+    """THyMe's own dataset and shipped results (delta = 86,400,000): the
+    dataset has ties in time, which THyMe breaks at random, so the check is
+    on what ties cannot change: the total and the sum per static class, which
+    all three of THyMe's exact programs agree on."""
+    rec = load_golden("temporal")["email-Enron"]
+    p = refdata.path("email-Enron")
+    if p is None:
+        pytest.skip("reference dataset not present (oracle/build_ref.sh copies it)")
+    assert refdata.sha256(p) == rec["file_sha256"]
+    off, mem, times, _ = refdata.read_thyme(p)
+    got = oracle.temporal96(off, mem, times, rec["delta"])
+    assert int(got.sum()) == rec["total"] == 127357
+    assert refdata.per_static(got) == rec["per_static"]
+    for k in ("thyme", "thymeP", "dp"):  # the fixture agrees with every shipped result file
+        rp = refdata.path(f"email-Enron-{k}")
+        if rp is not None:
+            assert refdata.per_static(refdata.read_thyme_result(rp)[1]) == rec["per_static"]
 
 
 @pytest.mark.parametrize("seed", range(6))

@@ -1,7 +1,8 @@
 """The reference-shaped C++ shim (include/hmotif_cbst.hpp) run on the GPU: a
 program written against the reference's host interface (flat 1-based
 payloads with 0 pads, 1-based keys, computeMotifCounts, an erase + insert
-batch with its delta, the three-layer temporal ring and its delta file)
+batch with its delta, keyed insert (fillCBST) and unfill with their deltas,
+the three-layer temporal ring and its delta file)
 prints counts that equal the oracle's."""
 import re
 import shutil
@@ -58,6 +59,16 @@ int main(int argc, char** argv) {
   std::printf("keys: %d %d\n", keys[0], keys[1]);
   c = hm::computeMotifCounts(store, false);
   print("after", std::vector<int64_t>(c.begin(), c.end()));
+  // CBSTOperations::insert(insertKeys, insertPayload, insertPrefixSizes) is
+  // fillCBST: values appended to existing keys, which keep their ids
+  store.insert({1, 2}, {maxv, 3, 1}, {2, 3}, &d);
+  print("fill_delta", d);
+  c = hm::computeMotifCounts(store, false);
+  print("after_fill", std::vector<int64_t>(c.begin(), c.end()));
+  store.unfill({1}, {maxv}, {1}, &d);
+  print("unfill_delta", d);
+  c = hm::computeMotifCounts(store, false);
+  print("after_unfill", std::vector<int64_t>(c.begin(), c.end()));
 
   std::vector<int> tkeys;
   for (int i = 0; i < n; ++i) tkeys.push_back(i + 1);
@@ -123,6 +134,18 @@ def test_reference_shaped_program_matches_oracle(tmp_path):
     assert _line(out, "after") == after.tolist()
     assert _line(out, "delta") == (after.astype(np.int64) - before.astype(np.int64)).tolist()
     assert _line(out, "keys") == [n - 2, n - 1]  # freed keys reused, ascending
+    # keyed fill of keys 1 and 2, then unfill of key 1 (keys are 1-based)
+    filled = [list(r) for r in after_rows]
+    filled[0] = sorted(set(filled[0]) | {maxv, 3})
+    filled[1] = sorted(set(filled[1]) | {1})
+    after_fill = oracle.static30(*_csr(filled), maxv + 1)
+    assert _line(out, "after_fill") == after_fill.tolist()
+    assert _line(out, "fill_delta") == (after_fill.astype(np.int64) - after.astype(np.int64)).tolist()
+    unfilled = [list(r) for r in filled]
+    unfilled[0] = sorted(set(unfilled[0]) - {maxv})
+    after_unfill = oracle.static30(*_csr(unfilled), maxv + 1)
+    assert _line(out, "after_unfill") == after_unfill.tolist()
+    assert _line(out, "unfill_delta") == (after_unfill.astype(np.int64) - after_fill.astype(np.int64)).tolist()
 
     # the window: vertex v is node v - 1 in constructs, fills and delta files alike
     layer = [[v - 1 for v in r] for r in rows]

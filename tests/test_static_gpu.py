@@ -5,7 +5,7 @@ from math import comb
 import numpy as np
 import pytest
 
-from oracle import oracle
+from oracle import oracle, refdata
 from tests.helpers import csr, digest, load_golden, random_graph, static_case
 
 pytestmark = pytest.mark.gpu
@@ -19,6 +19,21 @@ def test_static_matches_mochy_golden(ctx, name):
     h = static_case(rec["params"])
     assert digest(h) == rec["sha256"]
     with engine.Graph.from_hypergraph(ctx, h) as g:
+        assert g.count_static().tolist() == rec["counts26"]
+
+
+def test_static_on_mochy_dblp(ctx):
+    """MoCHy's own sample hypergraph (dblp_graph.txt) against the counts
+    MoCHy main_exact printed for it."""
+    from ipdps26_b200 import engine
+
+    rec = load_golden("static")["dblp"]
+    p = refdata.path("dblp")
+    if p is None:
+        pytest.skip("reference dataset not present (oracle/build_ref.sh copies it)")
+    assert refdata.sha256(p) == rec["file_sha256"]
+    off, mem, n_nodes = refdata.read_mochy(p)
+    with engine.Graph(ctx, off, mem, n_nodes) as g:
         assert g.count_static().tolist() == rec["counts26"]
 
 
@@ -143,3 +158,51 @@ def test_async_count_on_caller_and_context_streams(ctx):
         for o in outs:
             assert o.cpu().numpy().view(np.uint64).tolist() == want.tolist()
         assert g.count_static30().tolist() == want.tolist()
+
+
+def test_async_count_on_the_default_stream_without_synchronize(ctx):
+    """Stream 0 (the legacy default stream, torch's default stream) is a
+    caller's stream like any other: a fill queued on it before the count, and
+    the read queued after it, are ordered with no explicit synchronize. The
+    phase times of an asynchronous count read as not measured."""
+    import torch
+
+    from ipdps26_b200 import engine, gen
+
+    h = gen.static(gen.config1(seed=79, n_nodes=700, n_edges=1400))
+    want = oracle.static30(h.offsets, h.members, h.n_nodes)
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        g.count_static30()  # prepared; later counts replay the captured launches
+        for _ in range(3):
+            out = torch.empty(30, dtype=torch.int64, device="cuda:0")
+            out.fill_(-1)
+            g.count_static30_async(out.data_ptr(), 0)
+            assert out.cpu().numpy().view(np.uint64).tolist() == want.tolist()
+        assert g.timings().closed_ms == -1.0
+
+
+def test_async_count_refuses_a_capturing_stream(ctx):
+    """A caller's stream under CUDA-graph capture is refused with
+    HM_ERR_STATE; the capture itself stays usable."""
+    import torch
+
+    from ipdps26_b200 import engine, gen
+    from ipdps26_b200._lib import HmError
+
+    h = gen.static(gen.config1(seed=80, n_nodes=300, n_edges=500))
+    with engine.Graph.from_hypergraph(ctx, h) as g:
+        g.count_static30()
+        out = torch.zeros(30, dtype=torch.int64, device="cuda:0")
+        s = torch.cuda.Stream(device=0)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with pytest.raises(HmError) as ei:
+                with torch.cuda.graph(graph, stream=s):
+                    out.add_(1)
+                    try:
+                        g.count_static30_async(out.data_ptr(), s.cuda_stream)
+                    finally:
+                        out.add_(1)
+        assert ei.value.status == -7
+        torch.cuda.synchronize()
+        assert g.count_static30().tolist() == oracle.static30(h.offsets, h.members, h.n_nodes).tolist()
