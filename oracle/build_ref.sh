@@ -31,6 +31,20 @@ if [ -d "$TD/src" ]; then
     $CXX -O2 -std=c++17 -DHM_TYPE=$t -I"$TD" -o "$OUT/type$t" "$HERE/ref_types.cpp" "$TD/src/graphGeneration.cpp" \
       "$TD/utils/utils.cpp" "$TD/utils/printUtils.cpp" "$TD/utils/flatten.cpp"
   done
+  # The reference's strictly increasing temporal counter (CUDA) with its store,
+  # through the harness ref_strictinc.cu -> _ref/strictinc (sm_100a).
+  # operations.cu uses std::sort without including <algorithm>; the header is
+  # pre-included rather than the source changed.
+  NVCC=${NVCC:-$(command -v nvcc || echo /usr/local/cuda/bin/nvcc)}
+  if [ -x "$NVCC" ]; then
+    "$NVCC" -std=c++17 -O2 -gencode arch=compute_100a,code=sm_100a --pre-include algorithm \
+      -I"$TD/include" -I"$TD/kernel" \
+      -o "$OUT/strictinc" "$HERE/ref_strictinc.cu" "$TD/src/temporal_count.cu" "$TD/src/temporal_structure.cpp" \
+      "$TD/structure/operations.cu" "$TD/kernel/insert_reuse.cu" "$TD/kernel/unfill.cu" "$TD/kernel/payload.cu" \
+      "$TD/kernel/build_tree.cu" "$TD/kernel/delete_avail.cu" "$TD/kernel/find.cu" "$TD/utils/flatten.cpp" \
+      "$TD/utils/utils.cpp" "$TD/utils/printUtils.cpp" "$TD/src/graphGeneration.cpp" 2>/dev/null ||
+      echo "build_ref.sh: the strict-increasing counter did not build; its parity test will skip" >&2
+  fi
 fi
 # The reference's own datasets with known outputs, copied verbatim for the
 # parity tests (refdata.py): MoCHy's dblp sample and THyMe's email-Enron with

@@ -96,3 +96,57 @@ def test_bad_inputs_change_nothing(ctx, tmp_path):
         with pytest.raises(HmError):
             w.apply_deltas_file(p)
         assert w.count30().tolist() == before
+
+
+REF_STRICTINC = __import__("pathlib").Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "strictinc"
+
+
+def _reference_layers(seed, sizes=(1, 2, 3, 5, 6, 7)):
+    """Three random layers inside the reference counter's own limits: no
+    hyperedge size a multiple of 4 (its payload then lacks an end marker)
+    and few enough hyperedges that no middle one has 1024 candidates."""
+    rng = np.random.default_rng(seed)
+    n_nodes = int(rng.integers(12, 45))
+    layers = []
+    for _ in range(3):
+        m = int(rng.integers(20, 120))
+        rows = [sorted(rng.choice(n_nodes, size=min(int(rng.choice(sizes)), n_nodes), replace=False).tolist())
+                for _ in range(m)]
+        layers.append(rows)
+    return n_nodes, layers
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_strictinc_matches_the_reference_counter(ctx, seed, tmp_path):
+    """The reference's own temporalStrictIncAdjKernel (built from its sources
+    into oracle/_ref/strictinc by build_ref.sh, run on this GPU) against
+    hm_window_count30 and the oracle, bin for bin."""
+    import subprocess
+
+    from ipdps26_b200 import engine
+    from oracle import oracle
+
+    if not REF_STRICTINC.exists():
+        pytest.skip("reference counter not built (oracle/build_ref.sh needs the reference tree and nvcc)")
+    n_nodes, layers = _reference_layers(seed)
+    f = tmp_path / "layers.txt"
+    with open(f, "w") as fh:  # vertices are 1-based in the reference's stores
+        fh.write(f"{n_nodes}\n")
+        for rows in layers:
+            fh.write(f"{len(rows)}\n")
+            for r in rows:
+                fh.write(f"{len(r)} {' '.join(str(v + 1) for v in r)}\n")
+    r = subprocess.run([str(REF_STRICTINC), str(f)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("strictinc30:")]
+    assert line, r.stdout[-2000:]
+    ref = [int(x) for x in line[-1].split()[1:]]
+    assert len(ref) == 30
+    csrs = [_csr(rows) for rows in layers]
+    with engine.Window(ctx, n_nodes) as w:
+        for l, (off, mem) in enumerate(csrs):
+            w.set_layer(l, off, mem)
+        got = w.count30()
+    assert sum(ref) > 0
+    assert got.tolist() == ref
+    assert oracle.strictinc30(csrs).tolist() == ref
