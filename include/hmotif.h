@@ -144,6 +144,12 @@ int hm_debug_fail_allocations_after(long long n);
  * 1 = its higher-id neighbours, read straight from the id-sorted rows (what
  * pooled server stores use). Counts are the same either way; tests run both. */
 int hm_debug_touch_orientation(hm_graph* g, int by_id);
+/* Walk of the static count on graph g: 1 (the default) walks oriented rows
+ * grouped by the member each neighbour shares with the row owner, and counts
+ * the triangles of a pair sharing one member u through the neighbours that
+ * share only u by the group's size counts instead of visiting them; 0 visits
+ * every oriented entry. Counts are the same either way; tests run both. */
+int hm_debug_static_groups(hm_graph* g, int on);
 
 /* ---- the device store ------------------------------------------------- */
 /* Builds H2V (hyperedge -> sorted members), V2H (node -> sorted hyperedges)
@@ -268,8 +274,12 @@ int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, uint32_t n, 
  * timestamps) for the window delta: every event a and the connected triples
  * of the projection of the events with t_a - delta <= t <= t_a that contain
  * it, repeated node-sets collapsed into one hyperedge with several
- * occurrences (THyMe-main/code/main_thymeP.cpp:155-368). Equal timestamps are
- * ordered by input position. HM_ERR_LIMIT if an event has more than 2048
+ * occurrences (THyMe-main/code/main_thymeP.cpp:155-368). Events with equal
+ * timestamps are processed in input order; the order of two occurrences is
+ * decided by a strict comparison of their times, as THyMe compares them
+ * (main_thymeP.cpp:313-323), a tie counting as "c before b" with b the
+ * hyperedge of the pair whose node-set comes first in the input (THyMe's own
+ * numbering, which its input shuffle randomises). HM_ERR_LIMIT if an event has more than 2048
  * distinct neighbours inside its window. There is no temporal counter of
  * these 96 motifs in the reference's GPU code (its 3-layer strict-increasing
  * kernel, temporalDynamicHMotif/src/temporal_count.cu:91-217, bins 30 classes

@@ -363,6 +363,14 @@ extern "C" int hm_graph_temporal_traffic(const hm_graph* g, hm_temporal_traffic_
   return HM_OK;
 }
 
+extern "C" int hm_debug_static_groups(hm_graph* g, int on) {
+  if (!g) return hm::set_error(HM_ERR_INVALID, "hm_debug_static_groups: NULL graph");
+  CtxLock lock(g->ctx);
+  g->use_groups = on != 0;
+  if (!g->use_groups) hm::release_plus_groups(g);
+  return HM_OK;
+}
+
 extern "C" int hm_debug_touch_orientation(hm_graph* g, int by_id) {
   if (!g) return hm::set_error(HM_ERR_INVALID, "hm_debug_touch_orientation: NULL graph");
   g->touch_by_id = by_id != 0;

@@ -111,7 +111,7 @@ struct TouchSchedule {
 // Launch sequences of the static count captured as CUDA graphs (open phase,
 // closed phase), replayed while the arguments they were captured with hold.
 struct CountCapture {
-  static constexpr unsigned kKey = 20;
+  static constexpr unsigned kKey = 27;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   uint64_t key[kKey] = {};
   bool valid = false;
@@ -177,6 +177,21 @@ struct hm_graph {
   hm::DArr<uint16_t> plus_os;  // (neighbour size << 8) | overlap
   hm::DArr<uint64_t> plus_mask;
   uint64_t plus_nnz = 0;
+  // The oriented rows once more, grouped for the static count's walk: in
+  // each row, first the neighbours that share several members with the row
+  // owner (or one at a position past 63 of its member list), then one group
+  // per position p < 64 holding the neighbours whose only shared member is
+  // the owner's p-th. Per row a group table: group starts relative to the
+  // row (min(size, 64) + 2 entries, the last the row length) and, per group,
+  // how many of its neighbours have one and two members.
+  bool grp_valid = false;
+  bool use_groups = true;  // hm_debug_static_groups: off walks every entry (same counts)
+  hm::DArr<uint32_t> grp_nbr;
+  hm::DArr<uint16_t> grp_os;
+  hm::DArr<uint64_t> grp_base;   // per slot: its group table's first entry
+  hm::DArr<uint32_t> grp_start;
+  hm::DArr<uint32_t> grp_one;    // neighbours of size 1 in the group
+  hm::DArr<uint32_t> grp_two;    // neighbours of size 2 in the group
 
   // static-count state that only changes with the graph
   bool work_valid = false;
@@ -224,6 +239,8 @@ int build_h2h_rows(hm_graph* g);
 int h2h_rows_for(hm_graph* g, const uint32_t* d_rows, uint32_t n_rows,
                  const std::function<int(uint64_t, uint64_t*)>& reserve, uint64_t* written);
 int build_plus(hm_graph* g);
+int build_plus_groups(hm_graph* g);
+void release_plus_groups(hm_graph* g);
 // Oriented rows of a subset of slots (indexed by slot; only listed slots valid).
 struct PlusRows {
   DArr<uint64_t> off;
@@ -323,6 +340,15 @@ struct StreamOrder {
     return HM_OK;
   }
 };
+
+#ifdef __CUDACC__
+// The orientation of the oriented rows: b is "above" a when (deg b, b) >
+// (deg a, a), deg the H2H degree; every triangle is found once, from its
+// lowest-ranked corner, and hub rows stay short.
+__device__ __forceinline__ bool rank_above(uint32_t a, uint32_t da, uint32_t b, uint32_t db) {
+  return db > da || (db == da && b > a);
+}
+#endif
 
 inline unsigned grid_for(uint64_t items, unsigned per_block, unsigned max_blocks = 148u * 32u) {
   uint64_t b = (items + per_block - 1) / per_block;

@@ -157,7 +157,23 @@ struct ClosedArgs {
   uint8_t* edge_flags;      // diagnostics only: marks oriented entries that close a triangle
   const uint32_t* gos;      // per slot: its graph (null: one output row)
   const uint32_t* rog;      // per graph: output row
+  // The grouped copy of the oriented rows walked as N+(b) (hm_graph::grp_nbr;
+  // null: walk pnbr / pos, no group is skipped) and the (degree, id) rank.
+  const uint32_t* wnbr;
+  const uint16_t* wos;
+  const uint64_t* wbase;
+  const uint32_t* wstart;
+  const uint32_t* wone;
+  const uint32_t* wtwo;
+  const uint32_t* hdeg;     // H2H degree per slot: the orientation's rank
 };
+
+// Heavy neighbours (sharing two or more members) of a centre kept in shared
+// memory for the skipped-group correction; a centre with more walks every
+// group.
+constexpr uint32_t kHeavyBlock = 96;  // per block-per-centre table
+constexpr uint32_t kHeavyWarp = 16;   // per warp-per-centre table
+constexpr uint32_t kGroupPositions = 64;
 
 // |a & b & c| by a three-way merge of the member lists (centres with more
 // than 64 members, whose position masks are incomplete).
@@ -208,17 +224,30 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
 // One value per key: the shared-position mask when the centre has at most 64
 // members (its overlap is then the mask's popcount), else the overlap; the
 // row index in the diagnostic pass.
+// With skip set (a centre of at most 64 members whose heavy neighbours all fit
+// hv_c / hv_m, and grouped rows to walk), the walk of N+(b) for a b sharing a
+// single member u with a leaves out b's group of neighbours sharing only u:
+// those triangles are counted per size category from the group's counts,
+// and the few of them that are not stars (they overlap a in two or more
+// members) are found in the centre's heavy list.
 struct CentreTable {
   const uint32_t* keys;
   const uint64_t* sval;
   uint32_t shift, bmask;
   bool in_smem;
+  const uint32_t* hv_c;  // heavy neighbours of the centre in N+(a) ...
+  const uint64_t* hv_m;  // ... and their shared-position masks
+  uint32_t hv_n;
+  bool skip;
 };
 
-// Fills the table with N+(a), threads t = first, first + stride, ...
+// Fills the table with N+(a), threads t = first, first + stride, ...; the
+// entries sharing two or more members with a also go to the heavy list while
+// it has room (*hv_n counts them all).
 __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys,
                                            uint64_t* sval, uint32_t shift, uint32_t bmask, bool flags, bool exact,
-                                           unsigned first, unsigned stride) {
+                                           unsigned first, unsigned stride, uint32_t* hv_c, uint64_t* hv_m,
+                                           uint32_t* hv_n, uint32_t hv_max) {
   for (uint32_t i = first; i < ad; i += stride) {
     const uint32_t key = A.pnbr[ao + i];
     uint32_t bk = hash_slot(key, shift), h = 0;
@@ -229,8 +258,45 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
           done = true;
           break;
         }
-    sval[h] = flags ? (uint64_t)i : exact ? A.pmask[ao + i] : (uint64_t)(A.pos[ao + i] & 0xffu);
+    const uint64_t m = exact ? A.pmask[ao + i] : 0;
+    sval[h] = flags ? (uint64_t)i : exact ? m : (uint64_t)(A.pos[ao + i] & 0xffu);
+    if (hv_n && exact && (A.pos[ao + i] & 0xffu) >= 2u) {
+      const uint32_t k = atomicAdd(hv_n, 1u);
+      if (k < hv_max) {
+        hv_c[k] = key;
+        hv_m[k] = m;
+      }
+    }
   }
+}
+
+// Whole warp, converged: the lanes with push set append their record to the
+// warp's queue (64 places); every full 32 are classified at once.
+__device__ __forceinline__ void queue_push(bool push, uint64_t rec, uint64_t* q, uint32_t& qn, uint32_t sa,
+                                           unsigned long long* wc) {
+  const unsigned lane = lane_id();
+  const unsigned bal = __ballot_sync(0xffffffffu, push);
+  if (push) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+  qn += (uint32_t)__popc(bal);
+  if (qn >= kWarp) {
+    __syncwarp();
+    classify_queue(q, kWarp, sa, wc);
+    if (lane < qn - kWarp) q[lane] = q[kWarp + lane];
+    __syncwarp();
+    qn -= kWarp;
+  }
+}
+
+// Number of shared members of two sorted lists, counting no further than 2.
+__device__ __forceinline__ uint32_t shared_upto2(const uint32_t* x, uint32_t nx, const uint32_t* y, uint32_t ny) {
+  uint32_t i = 0, j = 0, c = 0;
+  while (i < nx && j < ny && c < 2) {
+    const uint32_t u = x[i], v = y[j];
+    c += u == v;
+    i += u <= v;
+    j += v <= u;
+  }
+  return c;
 }
 
 // One whole warp: walks N+(b) for the bi-th entry b of N+(a), probes the
@@ -256,20 +322,78 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   const uint64_t mab = A.pmask[ao + bi];
   const uint64_t bo = A.poff[b];
   const uint32_t bd = A.plen[b];
+  // N+(b) is walked in its grouped copy when there is one (any order of a
+  // row's entries finds the same triangles); the diagnostic pass walks the
+  // id-sorted rows, whose entry indices it records.
+  const bool grouped = A.wnbr != nullptr && !flags;
+  const uint32_t* wnbr = grouped ? A.wnbr : A.pnbr;
+  const uint16_t* wos = grouped ? A.wos : A.pos;
   uint32_t star0 = 0, star1 = 0, star2 = 0;
   unsigned long long triads = 0;
+  // The group of b's neighbours whose only shared member with b is u, the
+  // only member a and b share, is left out of the walk: each of them closes
+  // a triangle {a, b, c} through u. They are counted as stars by the size of
+  // c (lane 0 holds the group's counts), and the ones that share two or more
+  // members with a, all in a's heavy list, are taken back out and queued as
+  // the non-star triangles they are (C_ab = C_bc = 1, g = 1).
+  uint32_t gs = 0, glen = 0;
+  if (!kTriads && T.skip && grouped && cab == 1) {
+    const uint32_t qu = (uint32_t)(__ffsll((long long)mab) - 1);  // u's position in a (a has <= 64 members)
+    const uint32_t u = A.hmem[A.hoff[a] + qu];
+    const uint32_t* bm = A.hmem + A.hoff[b];
+    uint32_t lo = 0, hi = sb;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (bm[mid] < u) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < kGroupPositions) {  // u's position in b; past 63 its entries sit in group 0 and are walked
+      const uint64_t t = A.wbase[b] + 1 + lo;
+      gs = A.wstart[t];
+      glen = A.wstart[t + 1] - gs;
+      if (lane == 0) {
+        star0 = A.wone[t];
+        star1 = A.wtwo[t];
+        star2 = glen - star0 - star1;
+      }
+      const uint32_t db = A.hdeg[b];
+      for (uint32_t k0 = 0; k0 < T.hv_n; k0 += kWarp) {
+        const uint32_t k = k0 + lane;
+        bool push = false;
+        uint64_t rec = 0;
+        if (k < T.hv_n) {
+          const uint64_t mac = T.hv_m[k];
+          const uint32_t c = T.hv_c[k];
+          if (((mac >> qu) & 1ull) && rank_above(b, db, c, A.hdeg[c])) {
+            const uint32_t sc = A.esize[c];
+            if (shared_upto2(bm, sb, A.hmem + A.hoff[c], sc) == 1) {  // b & c = {u}: in the skipped group
+              const uint32_t cc = size_cat(sc);
+              star0 -= cc == 0;  // per-lane counters summed modulo 2^32 below
+              star1 -= cc == 1;
+              star2 -= cc == 2;
+              push = true;
+              rec = pack_triangle(sb, sc, 1, 1, (uint32_t)__popcll(mac), 1);
+            }
+          }
+        }
+        queue_push(push, rec, q, qn, sa, wc);
+      }
+    }
+  }
+  const uint32_t bdw = bd - glen;  // entries walked
   // kUnroll probes per lane per round: their id and overlap/size loads are
   // issued together so several global loads are in flight per lane.
-  for (uint32_t j0 = 0; j0 < bd; j0 += kWarp * kUnroll) {
+  for (uint32_t j0 = 0; j0 < bdw; j0 += kWarp * kUnroll) {
     uint32_t cv[kUnroll], ov[kUnroll];
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
       const uint32_t j = j0 + u * kWarp + lane;
       cv[u] = kEmpty;
       ov[u] = 0;
-      if (j < bd) {
-        cv[u] = __ldg(A.pnbr + bo + j);
-        ov[u] = __ldg(A.pos + bo + j);
+      if (j < bdw) {
+        const uint32_t jj = j < gs ? j : j + glen;
+        cv[u] = __ldg(wnbr + bo + jj);
+        ov[u] = __ldg(wos + bo + jj);
       }
     }
 #pragma unroll
@@ -349,18 +473,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
       push = true;
       rec = pack_triangle(sb, sc, cab, cbc, cac, g);
       } while (false);
-      if (!kTriads) {  // warp-converged: queue this slice's triangles (64 places)
-        const unsigned bal = __ballot_sync(0xffffffffu, push);
-        if (push) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
-        qn += (uint32_t)__popc(bal);
-        if (qn >= kWarp) {
-          __syncwarp();
-          classify_queue(q, kWarp, sa, wc);
-          if (lane < qn - kWarp) q[lane] = q[kWarp + lane];
-          __syncwarp();
-          qn -= kWarp;
-        }
-      }
+      if (!kTriads) queue_push(push, rec, q, qn, sa, wc);  // warp-converged
     }
   }
   if (kTriads) {
@@ -407,7 +520,9 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kHashSlotsMax);  // kHashSlotsMax
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];  // per warp: triangles waiting to be classified
-  __shared__ uint32_t s_item;
+  __shared__ uint32_t hv_c[kHeavyBlock];
+  __shared__ uint64_t hv_m[kHeavyBlock];
+  __shared__ uint32_t s_item, hv_n;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
   uint64_t* q = wqueue[w];
@@ -416,7 +531,10 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   uint32_t cur_row = kNoRow;  // per-request rows: the row wc is collecting for
 
   for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(A.queue, 1u);
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(A.queue, 1u);
+      hv_n = 0;
+    }
     __syncthreads();
     const uint64_t item = (uint64_t)s_item * A.n_shards + A.shard;
     if (item >= A.n_work) break;
@@ -432,7 +550,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t ad = A.plen[a];
     const uint32_t sa = A.esize[a];
     const bool flags = A.edge_flags != nullptr;
-    CentreTable T{keys, sval, 32, 0, ad <= kHashRowMax};
+    CentreTable T{keys, sval, 32, 0, ad <= kHashRowMax, hv_c, hv_m, 0, false};
     if (T.in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
@@ -441,11 +559,14 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x);
+      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x, hv_c, hv_m,
+                 &hv_n, kHeavyBlock);
     }
     __syncthreads();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
+    T.hv_n = hv_n;
+    T.skip = T.in_smem && exact_masks && !flags && A.wnbr && T.hv_n <= kHeavyBlock;
     for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
       closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
@@ -469,6 +590,9 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
   __shared__ uint64_t val_all[kClosedWarps][kWarpSlots];
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];
+  __shared__ uint32_t hvc_all[kClosedWarps][kHeavyWarp];
+  __shared__ uint64_t hvm_all[kClosedWarps][kHeavyWarp];
+  __shared__ uint32_t hvn_all[kClosedWarps];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint32_t* keys = keys_all[w];
   uint64_t* sval = val_all[w];
@@ -499,13 +623,18 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     uint32_t slots = 64;
     while (slots < 2 * ad && slots < kWarpSlots) slots <<= 1;
     const uint32_t buckets = slots / 4;
-    CentreTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true};
+    CentreTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true, hvc_all[w], hvm_all[w], 0,
+                  false};
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
+    if (lane == 0) hvn_all[w] = 0;
     __syncwarp();
-    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp);
+    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp, hvc_all[w], hvm_all[w],
+               &hvn_all[w], kHeavyWarp);
     __syncwarp();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
+    T.hv_n = hvn_all[w];
+    T.skip = exact_masks && !flags && A.wnbr && T.hv_n <= kHeavyWarp;
     for (uint32_t bi = 0; bi < ad; ++bi) {
       closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
@@ -627,6 +756,19 @@ static int prepare_static_attrs() {
   return HM_OK;
 }
 
+// The grouped rows and the rank the closed phase's walk uses (left null,
+// the walk takes the id-sorted rows and skips nothing).
+static void with_groups(const hm_graph* g, ClosedArgs& A) {
+  if (!g->use_groups || !g->grp_valid) return;
+  A.wnbr = g->grp_nbr.p;
+  A.wos = g->grp_os.p;
+  A.wbase = g->grp_base.p;
+  A.wstart = g->grp_start.p;
+  A.wone = g->grp_one.p;
+  A.wtwo = g->grp_two.p;
+  A.hdeg = g->h2h_len.p;
+}
+
 // Everything the count kernels need that only changes with the graph.
 int prepare_static(hm_graph* g) {
   hm_ctx* ctx = g->ctx;
@@ -634,6 +776,7 @@ int prepare_static(hm_graph* g) {
     HM_TRY(build_plus(g));
     g->work_valid = false;
   }
+  if (g->use_groups && !g->grp_valid) HM_TRY(build_plus_groups(g));
   if (!g->work_valid && g->n_slots) HM_TRY(closed_worklist(g));
   if (!g->counters.p) HM_TRY(g->counters.alloc(ctx, 64));
   if (!g->ev_ready) {
@@ -706,10 +849,11 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  const ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
-                        g->h2v_off.p,  g->h2v_mem.p,  g->esize.p,    g->work.p,    0,
-                        shard,         n_shards,      nullptr,       dev,          edge_flags,
-                        nullptr,       nullptr};
+  ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
+                  g->h2v_off.p,  g->h2v_mem.p,  g->esize.p,    g->work.p,    0,
+                  shard,         n_shards,      nullptr,       dev,          edge_flags,
+                  nullptr,       nullptr};
+  with_groups(g, args);
   auto open_phase = [&]() -> int {
     HM_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 48, st));
     if (E) {
@@ -736,7 +880,9 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
       (uint64_t)g->esize.p,    (uint64_t)g->plus_off.p, (uint64_t)g->plus_len.p,  (uint64_t)g->plus_nbr.p,
       (uint64_t)g->plus_os.p,  (uint64_t)g->plus_mask.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
       (uint64_t)g->work.p,     (uint64_t)dev,            E,                       g->n_work,
-      g->n_work_big,           g->n_work_mid,            shard,                   n_shards};
+      g->n_work_big,           g->n_work_mid,            shard,                   n_shards,
+      (uint64_t)args.wnbr,     (uint64_t)args.wos,       (uint64_t)args.wbase,    (uint64_t)args.wstart,
+      (uint64_t)args.wone,     (uint64_t)args.wtwo,      (uint64_t)args.hdeg};
   CountCapture& C = g->capture;
   bool same = C.valid;
   for (unsigned k = 0; k < CountCapture::kKey && same; ++k) same = C.key[k] == key[k];
@@ -1082,11 +1228,12 @@ int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report& R) {
       HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
       HM_CUDA(cudaStreamSynchronize(st));
       const uint32_t bounds[4] = {0, hw[1], hw[2], hw[0]};
+      ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p,
+                       g->h2v_mem.p,    g->esize.p,    work.p,         0,             0,               1,
+                       nullptr,         cnt.p,         nullptr,        nullptr,       nullptr};
+      with_groups(g, targs);
       HM_CUDA(cudaEventRecord(ev.e[0], st));
-      HM_TRY(launch_closed(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
-                                           g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, work.p, 0, 0, 1,
-                                           nullptr, cnt.p, nullptr, nullptr, nullptr},
-                           bounds, reinterpret_cast<unsigned int*>(cnt.p + 42)));
+      HM_TRY(launch_closed(ctx, targs, bounds, reinterpret_cast<unsigned int*>(cnt.p + 42)));
       HM_CUDA(cudaEventRecord(ev.e[1], st));
       HM_CUDA(cudaEventSynchronize(ev.e[1]));
       float ms = 0;

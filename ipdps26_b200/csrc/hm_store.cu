@@ -236,10 +236,8 @@ __global__ void k_chunk_emit(const int* beg, const int* end, const uint32_t* key
 
 // ---- oriented adjacency --------------------------------------------------------
 
-// b is "above" a when (deg b, b) > (deg a, a): every triangle is found once,
-// from its lowest-ranked corner, and hub rows stay short.
 __device__ __forceinline__ bool above(uint32_t a, uint32_t da, uint32_t b, uint32_t db) {
-  return db > da || (db == da && b > a);
+  return rank_above(a, da, b, db);
 }
 
 // rows == nullptr: rows 0..n-1; else the listed rows. cnt[i] is the i-th
@@ -292,7 +290,115 @@ __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uin
   }
 }
 
+// Groups per oriented row of owner b: group 0 the neighbours sharing several
+// members with b, or one at a position >= 64 of b's list (their position mask
+// is then empty); group 1 + p those whose only shared member is b's p-th.
+constexpr uint32_t kGroupPositions = 64;
+__device__ __forceinline__ uint32_t n_groups(uint32_t size) { return 1u + min(size, kGroupPositions); }
+__device__ __forceinline__ uint32_t group_of(uint16_t os, uint64_t mask) {
+  return ((os & 0xffu) == 1u && mask) ? 1u + (uint32_t)(__ffsll((long long)mask) - 1) : 0u;
+}
+
+__global__ void k_group_sizes(const uint8_t* esize, uint32_t n, uint32_t* tsize) {
+  for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < n; b += (uint64_t)gridDim.x * blockDim.x)
+    tsize[b] = n_groups(esize[b]) + 1;
+}
+
+// One warp per row: group histogram (and the size-1 / size-2 neighbours of
+// each group) in shared memory, its prefix sums as the group table, then a
+// scatter of the row's entries into the grouped copy.
+constexpr unsigned kGroupWarps = kBlock / kWarp;
+__global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, const uint32_t* plen,
+                                                       const uint32_t* pnbr, const uint16_t* pos,
+                                                       const uint64_t* pmask, const uint8_t* esize, uint32_t n,
+                                                       const uint64_t* gbase, uint32_t* gstart, uint32_t* gone,
+                                                       uint32_t* gtwo, uint32_t* gnbr, uint16_t* gos) {
+  __shared__ uint32_t cnt[kGroupWarps][kGroupPositions + 1];
+  __shared__ uint32_t one[kGroupWarps][kGroupPositions + 1];
+  __shared__ uint32_t two[kGroupWarps][kGroupPositions + 1];
+  const unsigned w = threadIdx.x / kWarp, lane = lane_id();
+  for (uint64_t b = global_warp(); b < n; b += n_warps()) {
+    const uint32_t G = n_groups(esize[b]);
+    for (uint32_t k = lane; k < G; k += kWarp) cnt[w][k] = one[w][k] = two[w][k] = 0;
+    __syncwarp();
+    const uint64_t s = poff[b];
+    const uint32_t l = plen[b];
+    for (uint32_t i = lane; i < l; i += kWarp) {
+      const uint16_t o = pos[s + i];
+      const uint32_t grp = group_of(o, pmask[s + i]);  // < G: a position bit p < min(size, 64)
+      atomicAdd(&cnt[w][grp], 1u);
+      const uint32_t sc = o >> 8;
+      if (sc == 1) atomicAdd(&one[w][grp], 1u);
+      if (sc == 2) atomicAdd(&two[w][grp], 1u);
+    }
+    __syncwarp();
+    const uint64_t t = gbase[b];
+    if (lane == 0) {
+      uint32_t run = 0;
+      for (uint32_t k = 0; k < G; ++k) {
+        const uint32_t c = cnt[w][k];
+        gstart[t + k] = run;
+        gone[t + k] = one[w][k];
+        gtwo[t + k] = two[w][k];
+        cnt[w][k] = run;  // becomes the group's write cursor
+        run += c;
+      }
+      gstart[t + G] = run;
+      gone[t + G] = gtwo[t + G] = 0;
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < l; i += kWarp) {
+      const uint16_t o = pos[s + i];
+      const uint32_t d = atomicAdd(&cnt[w][group_of(o, pmask[s + i])], 1u);
+      gnbr[s + d] = pnbr[s + i];
+      gos[s + d] = o;
+    }
+    __syncwarp();
+  }
+}
+
 }  // namespace
+
+// The grouped copy of the oriented rows (see hm_graph::grp_nbr).
+int build_plus_groups(hm_graph* g) {
+  hm_ctx* ctx = g->ctx;
+  cudaStream_t st = ctx->stream;
+  const uint32_t E = g->n_slots;
+  DArr<uint32_t> tsize;
+  HM_TRY(tsize.alloc(ctx, E));
+  HM_TRY(g->grp_base.alloc(ctx, (size_t)E + 1));
+  if (E) {
+    k_group_sizes<<<grid_for(E, kBlock), kBlock, 0, st>>>(g->esize.p, E, tsize.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(exclusive_scan(ctx, tsize.p, g->grp_base.p, E));
+  uint64_t tab = 0;
+  HM_CUDA(cudaMemcpyAsync(&tab, g->grp_base.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  HM_TRY(g->grp_start.alloc(ctx, tab));
+  HM_TRY(g->grp_one.alloc(ctx, tab));
+  HM_TRY(g->grp_two.alloc(ctx, tab));
+  HM_TRY(g->grp_nbr.alloc(ctx, g->plus_nnz));
+  HM_TRY(g->grp_os.alloc(ctx, g->plus_nnz));
+  if (E) {
+    k_group_rows<<<grid_for((uint64_t)E * kWarp, kBlock), kBlock, 0, st>>>(
+        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->esize.p, E, g->grp_base.p,
+        g->grp_start.p, g->grp_one.p, g->grp_two.p, g->grp_nbr.p, g->grp_os.p);
+    HM_LAUNCH_CHECK();
+  }
+  g->grp_valid = true;
+  return HM_OK;
+}
+
+void release_plus_groups(hm_graph* g) {
+  g->grp_nbr.release();
+  g->grp_os.release();
+  g->grp_base.release();
+  g->grp_start.release();
+  g->grp_one.release();
+  g->grp_two.release();
+  g->grp_valid = false;
+}
 
 struct WidenU64 {
   __host__ __device__ uint64_t operator()(uint32_t x) const { return x; }
@@ -641,6 +747,7 @@ int build_plus(hm_graph* g) {
   g->plus_len = static_cast<DArr<uint32_t>&&>(cnt);
   g->plus_nnz = total;
   g->plus_valid = true;
+  g->grp_valid = false;  // the grouped copy follows the rows it was built from
   return HM_OK;
 }
 

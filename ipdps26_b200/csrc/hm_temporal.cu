@@ -25,8 +25,14 @@
 //   3. open at b: c reaches b through a node outside a and c misses a;
 //      counted once per (b, c) at their smallest shared node;
 //   4. motifs 87-96 from the occurrence lists.
-// Ties in time are ordered by input index (THyMe's order among equal times is
-// random, so parity covers strictly increasing times).
+// Equal times. THyMe shuffles its input and then sorts by time, so its order
+// among equal times is random and its counts vary between runs. Here events
+// with equal times are processed in input order, and the rest follows THyMe
+// with its node-sets numbered in input order: of two occurrences, the one
+// strictly earlier in time comes first (main_thymeP.cpp:313-323), and a tie
+// counts as "c before b", where b is the node-set of the pair met first in
+// the input. The total and the per-static-class sums do not depend on any of
+// this; with strictly increasing times none of it arises.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -177,6 +183,7 @@ struct TArgs {
   const uint64_t* ooff;  // static id -> occurrence positions
   const uint32_t* olen;
   const uint32_t* opos;
+  const int64_t* tp;     // position -> time
   unsigned int* queue;
   unsigned long long* out;  // 96
   int* overflow;
@@ -205,13 +212,19 @@ __device__ __forceinline__ void range_in(const uint32_t* x, uint32_t n, uint32_t
   last = l;
 }
 
-// pairs (x in X, y in Y) with x < y, both sorted ascending
-__device__ __forceinline__ uint64_t ordered_pairs(const uint32_t* X, uint32_t nx, const uint32_t* Y, uint32_t ny) {
-  if (nx == 1 && ny == 1) return X[0] < Y[0];
+// Occurrence pairs (x in X, y in Y) with x strictly earlier in time than y,
+// X and Y positions sorted ascending (so their times are non-decreasing).
+// Times, not positions, are compared, as THyMe compares occurrence times
+// (THyMe-main/code/main_thymeP.cpp:313-323): two occurrences with equal
+// times count as "y before x", while the window itself follows positions.
+__device__ __forceinline__ uint64_t ordered_pairs(const int64_t* T, const uint32_t* X, uint32_t nx,
+                                                  const uint32_t* Y, uint32_t ny) {
+  if (nx == 1 && ny == 1) return T[X[0]] < T[Y[0]];
   uint64_t c = 0;
   uint32_t j = 0;
   for (uint32_t i = 0; i < nx; ++i) {
-    while (j < ny && Y[j] <= X[i]) ++j;
+    const int64_t tx = T[X[i]];
+    while (j < ny && T[Y[j]] <= tx) ++j;
     c += ny - j;
   }
   return c;
@@ -370,7 +383,11 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
         uint32_t cf, cl;
         range_in(co, A.olen[c], lo, p, cf, cl);
         const uint32_t nb = bl - bf, nc = cl - cf;
-        const uint64_t bc = ordered_pairs(bo + bf, nb, co + cf, nc);
+        // Of the two, the node-set that comes first in the input (the smaller
+        // static id) plays THyMe's "b": occurrence pairs with it strictly
+        // earlier go to its order, all others (ties too) to the other order.
+        const uint64_t bc = b < c ? ordered_pairs(A.tp, bo + bf, nb, co + cf, nc)
+                                  : (uint64_t)nb * nc - ordered_pairs(A.tp, co + cf, nc, bo + bf, nb);
         const uint64_t cb = (uint64_t)nb * nc - bc;
         const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, (int)cac, (int)cab, (int)g);
         const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, (int)cac, (int)g);
@@ -380,7 +397,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
       // 4. motifs 87-95 for the pair (a, b)
       if (lane == 0) {
         const uint32_t tb_n = bl - bf;
-        const uint64_t ab = ordered_pairs(ao + af, ta_n, bo + bf, tb_n);
+        const uint64_t ab = ordered_pairs(A.tp, ao + af, ta_n, bo + bf, tb_n);
         const uint64_t ba = (uint64_t)ta_n * tb_n - ab;
         const uint64_t bb = (uint64_t)tb_n * (tb_n ? tb_n - 1 : 0) / 2;
         const int kab = tclass((int)asz, (int)bsz, (int)asz, (int)cab, (int)cab, (int)asz, (int)cab);
@@ -439,7 +456,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
           uint32_t cf, cl;
           range_in(co, A.olen[c], lo, p, cf, cl);
           const uint32_t nb = bl - bf, nc = cl - cf;
-          const uint64_t bc = ordered_pairs(bo + bf, nb, co + cf, nc);
+          const uint64_t bc = ordered_pairs(A.tp, bo + bf, nb, co + cf, nc);
           const uint64_t cb = (uint64_t)nb * nc - bc;
           const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, 0, (int)cab, 0);
           const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, 0, 0);
@@ -601,7 +618,7 @@ static int launch_temporal(hm_graph* g, int64_t delta, DArr<uint32_t>& lo, DArr<
   k_window_lo<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_time.p, n, delta, lo.p);
   HM_LAUNCH_CHECK();
   TArgs A{n, g->t_order.p, g->t_static.p, g->t_prev.p, lo.p, g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
-          g->t_voff.p, g->t_vlen.p, g->t_vpos.p, g->t_ooff.p, g->t_olen.p, g->t_opos.p,
+          g->t_voff.p, g->t_vlen.p, g->t_vpos.p, g->t_ooff.p, g->t_olen.p, g->t_opos.p, g->t_time.p,
           reinterpret_cast<unsigned int*>(acc.p + 96), acc.p, reinterpret_cast<int*>(acc.p + 97), acc.p + 98};
   static bool attr = false;
   if (!attr) {

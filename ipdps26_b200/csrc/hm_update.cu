@@ -544,6 +544,7 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   g->plus_os.release();
   g->plus_mask.release();
   g->plus_valid = false;
+  release_plus_groups(g);
   HM_TRY(compact_h2h_in_place(g));
   const uint64_t live = g->h2h_tail;
   // keep at least half the live size free after a compaction, so that a
@@ -975,6 +976,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
   g->h2v_nnz = hs[1];
   g->plus_valid = false;
   g->work_valid = false;
+  release_plus_groups(g);  // rebuilt by the next static count; frees memory for the batches before it
 
   trace.mark("bookkeeping");
   if (hooks.after) {

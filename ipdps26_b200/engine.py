@@ -184,6 +184,7 @@ _lib.bind(
         "hm_graph_fill": (C.c_int, [vp, u32p, C.c_uint32, u32p, u64p, i64p]),
         "hm_graph_unfill": (C.c_int, [vp, u32p, C.c_uint32, u32p, u64p, i64p]),
         "hm_debug_touch_orientation": (C.c_int, [vp, C.c_int]),
+        "hm_debug_static_groups": (C.c_int, [vp, C.c_int]),
         "hm_count_vertex_triads": (C.c_int, [vp, u64p]),
         "hm_graph_set_schedule": (C.c_int, [vp, C.POINTER(Schedule)]),
         "hm_graph_get_schedule": (C.c_int, [vp, C.POINTER(Schedule)]),
@@ -435,6 +436,11 @@ class Graph:
         r = TuneReport()
         check(lib.hm_graph_autotune(self._h, int(sample_stride), C.byref(r)), "hm_graph_autotune")
         return r
+
+    def set_static_groups(self, on: bool) -> None:
+        """Walk of the static count: grouped rows with the shared-member group
+        counted in bulk (default), or every oriented entry (same counts)."""
+        check(lib.hm_debug_static_groups(self._h, int(on)), "hm_debug_static_groups")
 
     def set_touch_orientation(self, by_id: bool) -> None:
         """Walk order of the touched-triple counts (same counts either way)."""

@@ -500,8 +500,15 @@ int hmo_temporal96(uint32_t n_events, const uint64_t* offsets, const uint32_t* m
     rep[n_static] = e;
   }
   ++n_static;
-  /* 2. Events in time order (:188-195). Equal times are ordered by input
-   * position here; the reference shuffles them, so ties are outside parity. */
+  /* Input index of each node-set's first event: THyMe numbers node-sets in
+   * the order it meets them (:164-179), which decides which of two
+   * hyperedges of an instance is "b" when their occurrences tie in time. */
+  uint32_t* first_in = (uint32_t*)malloc(sizeof(uint32_t) * n_static);
+  for (uint32_t s = 0; s < n_static; ++s) first_in[s] = UINT32_MAX;
+  for (uint32_t e = 0; e < n_events; ++e)
+    if (first_in[sid[e]] == UINT32_MAX) first_in[sid[e]] = e;
+  /* 2. Events in time order (:188-195), equal times by input position (THyMe
+   * shuffles them, so its own counts vary between runs when times tie). */
   uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * n_events);
   for (uint32_t e = 0; e < n_events; ++e) order[e] = e;
   g_sort_t = times;
@@ -572,7 +579,8 @@ int hmo_temporal96(uint32_t n_events, const uint64_t* offsets, const uint32_t* m
       for (uint32_t k = 0; k < nb; ++k) {
         uint32_t c = nbr_c[k], sc = SS(c), cca = ovl_a[c];
         uint32_t cbc = inter_count(SM(b), sb, SM(c), sc);
-        if (cca && !(b < c)) continue; /* closed: once per unordered {b, c} */
+        /* closed: once per unordered {b, c}, b the node-set seen first in the input */
+        if (cca && !(first_in[b] < first_in[c])) continue;
         uint32_t g = cca ? inter3_count(SM(a), sa, SM(b), sb, SM(c), sc) : 0;
         uint32_t tc_n;
         COLLECT(c, tbuf_c, tc_n);
@@ -590,7 +598,11 @@ int hmo_temporal96(uint32_t n_events, const uint64_t* offsets, const uint32_t* m
         if (inter_count(SM(b), sb, SM(c), sc)) continue;
         uint32_t tc_n;
         COLLECT(c, tbuf_c, tc_n);
-        uint64_t bc = ordered_pairs(tbuf_b, tb_n, tbuf_c, tc_n);
+        /* the node-set seen first in the input takes THyMe's role of b: the
+         * occurrence pairs of b strictly before c go one way, the rest
+         * (ties included) the other */
+        uint64_t bc = first_in[b] < first_in[c] ? ordered_pairs(tbuf_b, tb_n, tbuf_c, tc_n)
+                                                : (uint64_t)tb_n * tc_n - ordered_pairs(tbuf_c, tc_n, tbuf_b, tb_n);
         uint64_t cb = (uint64_t)tb_n * tc_n - bc;
         int kbc = hmo_temporal_class((int)sb, (int)sc, (int)sa, 0, (int)cca, (int)cab, 0);
         int kcb = hmo_temporal_class((int)sc, (int)sb, (int)sa, 0, (int)cab, (int)cca, 0);
@@ -622,7 +634,7 @@ int hmo_temporal96(uint32_t n_events, const uint64_t* offsets, const uint32_t* m
   }
 #undef SM
 #undef SS
-  free(byset); free(sid); free(rep); free(order); free(occ_n); free(occ_first);
+  free(byset); free(sid); free(rep); free(order); free(occ_n); free(occ_first); free(first_in);
   free(tbuf_b); free(tbuf_c); free(win); free(nbr); free(nbr_c); free(mark); free(ovl_a);
   csr_free(&h);
   (void)cmp_edges_ctx_h;

@@ -206,3 +206,46 @@ def test_async_count_refuses_a_capturing_stream(ctx):
         assert ei.value.status == -7
         torch.cuda.synchronize()
         assert g.count_static30().tolist() == oracle.static30(h.offsets, h.members, h.n_nodes).tolist()
+
+
+def _heavy_rich_rows(rng):
+    """Hyperedges built so that the static count's grouped walk meets every
+    case: hubs 0 and 1 shared by 300 hyperedges (each pair shares both, so
+    centres have far more heavy neighbours than the shared-memory lists
+    hold), 400 hyperedges through hub 2 alone (light pairs: stars), a few
+    of 65-100 members whose members past position 63 are shared with small
+    hyperedges, size-1 and size-2 hyperedges on the hubs, and random ones."""
+    rows = [[0, 1, 10 + int(x)] for x in rng.choice(3000, size=300, replace=False)]
+    rows += [[2] + sorted(rng.choice(np.arange(4000, 9000), size=int(rng.integers(1, 5)), replace=False).tolist())
+             for _ in range(400)]
+    rows += [[2], [2], [0], [2, 5], [2, 6], [0, 1]]
+    for k in (65, 80, 100):
+        big = sorted(rng.choice(np.arange(9000, 9400), size=k, replace=False).tolist())
+        rows.append(big)
+        for p in (0, 30, 63, 64, k - 1):
+            rows.append([big[p], 9500 + int(rng.integers(0, 50))])
+        rows.append([big[70 % k], big[3], 2])
+    rows += [sorted(rng.choice(9600, size=int(rng.integers(2, 7)), replace=False).tolist()) for _ in range(800)]
+    return rows
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_grouped_walk_equals_plain_walk_and_oracle(ctx, seed):
+    """The static count with the shared-member groups counted in bulk (the
+    default) and with every oriented entry visited give the oracle's counts,
+    on a graph made to reach every branch of the grouped walk and on
+    config-2-law graphs, under the default and all-block schedules."""
+    from ipdps26_b200 import engine, gen
+
+    rng = np.random.default_rng(900 + seed)
+    cases = [(*csr(_heavy_rich_rows(rng)), 9700)]
+    h = gen.static(gen.config2(seed=40 + seed, n_nodes=4000, n_edges=8000, q=4.0))
+    cases.append((h.offsets, h.members, h.n_nodes))
+    for off, mem, n_nodes in cases:
+        want = oracle.static30(off, mem, n_nodes)
+        with engine.Graph(ctx, off, mem, n_nodes) as g:
+            for sched in ((128, 2048), (0, 0)):
+                g.set_schedule(*sched)
+                for on in (True, False, True):
+                    g.set_static_groups(on)
+                    assert g.count_static30().tolist() == want.tolist(), (sched, on)

@@ -87,3 +87,26 @@ def test_temporal_c4_laws(ctx):
         for delta in (1000, 10_000):
             want = oracle.temporal96(h.offsets, h.members, h.timestamps, delta)
             assert g.count_temporal(delta).tolist() == want.tolist(), delta
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_temporal_with_equal_times_matches_oracle(ctx, seed):
+    """Inputs where many events share a timestamp, and node-sets repeat: the
+    GPU and the oracle follow one tie rule (events in input order; a tie
+    between two occurrences counts as c before b, b the node-set met first
+    in the input), so all 96 counts agree."""
+    from ipdps26_b200 import engine
+
+    rng = np.random.default_rng(700 + seed)
+    for _ in range(25):
+        n_nodes = int(rng.integers(3, 10))
+        off, mem = random_graph(rng, int(rng.integers(3, 30)), n_nodes, 4)
+        rows = [mem[off[i]:off[i + 1]].tolist() for i in range(len(off) - 1)]
+        for i in range(0, len(rows), 3):
+            rows[i] = rows[max(0, i - 1)]
+        off, mem = csr(rows)
+        times = rng.integers(0, 5, size=len(rows)).astype(np.int64)
+        with engine.Graph(ctx, off, mem, n_nodes, times) as g:
+            for delta in (0, 1, 3, 10):
+                want = oracle.temporal96(off, mem, times, delta)
+                assert g.count_temporal(delta).tolist() == want.tolist(), (rows, times.tolist(), delta)
