@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--update-check-every", type=int, default=25,
                     help="full recount checking the running delta sum after every this many batches and after "
                          "the last (0: no check)")
+    ap.add_argument("--update-edits", type=int, default=0,
+                    help="edits per config-3 batch (0: log-uniform in [1000, 100000], as specified)")
+    ap.add_argument("--only", choices=["temporal", "update"], default=None,
+                    help="run one section alone on its own workload and print it (for profiling; no headline line)")
+    ap.add_argument("--temporal-deltas", default="1000,10000,100000")
     ap.add_argument("--no-temporal", action="store_true")
     ap.add_argument("--no-temporal-cpu", action="store_true")
     ap.add_argument("--temporal-samples", default="1000:50000,10000:10000,100000:1000",
@@ -247,6 +252,8 @@ def update_section(args, g, p, counts30):
     every = args.update_check_every
     for b in range(args.update_batches):
         n_edits = int(np.exp(rng.uniform(np.log(1_000), np.log(100_000))))
+        if args.update_edits:
+            n_edits = args.update_edits
         live = g.live_ids()
         dels, ins = gen.batch(p, 2_000_000 + b, live, n_edits, 0.8)
         t0 = time.perf_counter()
@@ -305,10 +312,9 @@ def temporal_section(args, ctx):
     h = gen.config4_temporal()
     res = {"events": h.n_edges, "workload": "config4 seed=3 200K nodes, Zipf(1.2), bursty span 1e8",
            "roofline_peak_gbs": hbm, "roofline_peak_kind": peak_kind}
-    samples = dict(temporal_samples(args))
     cores = os.cpu_count() or 1
     with engine.Graph.from_hypergraph(ctx, h) as g:
-        for d in (1_000, 10_000, 100_000):
+        for d in (int(x) for x in args.temporal_deltas.split(",")):
             c = g.count_temporal(d)
             ms = []
             for _ in range(3):
@@ -612,8 +618,28 @@ def engine_arm(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def section_only(args):
+    """One section on its own workload (for profiling one kernel family with
+    committed code): --only temporal (config 4 at --temporal-deltas) or
+    --only update (--update-batches of --update-edits on the workload at
+    --edges / --nodes)."""
+    from ipdps26_b200 import engine
+
+    with engine.Context(0) as ctx:
+        if args.only == "temporal":
+            out = temporal_section(args, ctx)
+        else:
+            p, h = workload(args)
+            with engine.Graph.from_hypergraph(ctx, h) as g:
+                out = update_section(args, g, p, g.count_static30())
+    print(json.dumps({"section": args.only, **out}), flush=True)
+
+
 def main():
     args = parse()
+    if args.only:
+        section_only(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -181,17 +181,18 @@ struct hm_graph {
   // each row, first the neighbours that share several members with the row
   // owner (or one at a position past 63 of its member list), then one group
   // per position p < 64 holding the neighbours whose only shared member is
-  // the owner's p-th. Per row a group table: group starts relative to the
-  // row (min(size, 64) + 2 entries, the last the row length) and, per group,
-  // how many of its neighbours have one and two members.
+  // the owner's p-th. Per row a group table of min(size, 64) + 2 entries
+  // {start relative to the row, neighbours of size 1, of size 2, 0}, the
+  // last one's start the row length. grp_opos follows the id-sorted oriented
+  // entries: for (a, b) sharing exactly one member, that member's position
+  // in b (0xff when they share several, or when it is past 63 in either).
   bool grp_valid = false;
   bool use_groups = true;  // hm_debug_static_groups: off walks every entry (same counts)
   hm::DArr<uint32_t> grp_nbr;
   hm::DArr<uint16_t> grp_os;
   hm::DArr<uint64_t> grp_base;   // per slot: its group table's first entry
-  hm::DArr<uint32_t> grp_start;
-  hm::DArr<uint32_t> grp_one;    // neighbours of size 1 in the group
-  hm::DArr<uint32_t> grp_two;    // neighbours of size 2 in the group
+  hm::DArr<uint4> grp_tab;
+  hm::DArr<uint8_t> grp_opos;
 
   // static-count state that only changes with the graph
   bool work_valid = false;

@@ -162,17 +162,11 @@ struct ClosedArgs {
   const uint32_t* wnbr;
   const uint16_t* wos;
   const uint64_t* wbase;
-  const uint32_t* wstart;
-  const uint32_t* wone;
-  const uint32_t* wtwo;
-  const uint32_t* hdeg;     // H2H degree per slot: the orientation's rank
+  const uint4* wtab;        // per group: {start in the row, size-1 neighbours, size-2 neighbours, 0}
+  const uint8_t* wopos;     // per oriented entry (a, b), id-sorted: position in b of the one member
+                            // a and b share, 0xff if they share several or it is past 63
 };
 
-// Heavy neighbours (sharing two or more members) of a centre kept in shared
-// memory for the skipped-group correction; a centre with more walks every
-// group.
-constexpr uint32_t kHeavyBlock = 96;  // per block-per-centre table
-constexpr uint32_t kHeavyWarp = 16;   // per warp-per-centre table
 constexpr uint32_t kGroupPositions = 64;
 
 // |a & b & c| by a three-way merge of the member lists (centres with more
@@ -224,30 +218,27 @@ __device__ __forceinline__ void add_star(unsigned long long* wc, uint32_t ca, ui
 // One value per key: the shared-position mask when the centre has at most 64
 // members (its overlap is then the mask's popcount), else the overlap; the
 // row index in the diagnostic pass.
-// With skip set (a centre of at most 64 members whose heavy neighbours all fit
-// hv_c / hv_m, and grouped rows to walk), the walk of N+(b) for a b sharing a
-// single member u with a leaves out b's group of neighbours sharing only u:
-// those triangles are counted per size category from the group's counts,
-// and the few of them that are not stars (they overlap a in two or more
-// members) are found in the centre's heavy list.
+// With skip set (a centre of at most 64 members, grouped rows to walk), the
+// walk of N+(b) for a b sharing a single member u with a may leave out b's
+// group of neighbours sharing only u: when no neighbour in N+(a) shares two
+// or more members with a including u (bit u of heavy_or clear), every entry
+// of that group is a star triangle {a, b, c}, counted per size category from
+// the group's counts.
 struct CentreTable {
   const uint32_t* keys;
   const uint64_t* sval;
   uint32_t shift, bmask;
   bool in_smem;
-  const uint32_t* hv_c;  // heavy neighbours of the centre in N+(a) ...
-  const uint64_t* hv_m;  // ... and their shared-position masks
-  uint32_t hv_n;
+  uint64_t heavy_or;  // OR of the shared-position masks of a's heavy neighbours in N+(a)
   bool skip;
 };
 
 // Fills the table with N+(a), threads t = first, first + stride, ...; the
-// entries sharing two or more members with a also go to the heavy list while
-// it has room (*hv_n counts them all).
+// masks of the entries sharing two or more members with a are ORed into
+// *heavy_or (when given).
 __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys,
                                            uint64_t* sval, uint32_t shift, uint32_t bmask, bool flags, bool exact,
-                                           unsigned first, unsigned stride, uint32_t* hv_c, uint64_t* hv_m,
-                                           uint32_t* hv_n, uint32_t hv_max) {
+                                           unsigned first, unsigned stride, unsigned long long* heavy_or) {
   for (uint32_t i = first; i < ad; i += stride) {
     const uint32_t key = A.pnbr[ao + i];
     uint32_t bk = hash_slot(key, shift), h = 0;
@@ -260,13 +251,7 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
         }
     const uint64_t m = exact ? A.pmask[ao + i] : 0;
     sval[h] = flags ? (uint64_t)i : exact ? m : (uint64_t)(A.pos[ao + i] & 0xffu);
-    if (hv_n && exact && (A.pos[ao + i] & 0xffu) >= 2u) {
-      const uint32_t k = atomicAdd(hv_n, 1u);
-      if (k < hv_max) {
-        hv_c[k] = key;
-        hv_m[k] = m;
-      }
-    }
+    if (heavy_or && exact && (A.pos[ao + i] & 0xffu) >= 2u) atomicOr(heavy_or, (unsigned long long)m);
   }
 }
 
@@ -285,18 +270,6 @@ __device__ __forceinline__ void queue_push(bool push, uint64_t rec, uint64_t* q,
     __syncwarp();
     qn -= kWarp;
   }
-}
-
-// Number of shared members of two sorted lists, counting no further than 2.
-__device__ __forceinline__ uint32_t shared_upto2(const uint32_t* x, uint32_t nx, const uint32_t* y, uint32_t ny) {
-  uint32_t i = 0, j = 0, c = 0;
-  while (i < nx && j < ny && c < 2) {
-    const uint32_t u = x[i], v = y[j];
-    c += u == v;
-    i += u <= v;
-    j += v <= u;
-  }
-  return c;
 }
 
 // One whole warp: walks N+(b) for the bi-th entry b of N+(a), probes the
@@ -331,52 +304,24 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   uint32_t star0 = 0, star1 = 0, star2 = 0;
   unsigned long long triads = 0;
   // The group of b's neighbours whose only shared member with b is u, the
-  // only member a and b share, is left out of the walk: each of them closes
-  // a triangle {a, b, c} through u. They are counted as stars by the size of
-  // c (lane 0 holds the group's counts), and the ones that share two or more
-  // members with a, all in a's heavy list, are taken back out and queued as
-  // the non-star triangles they are (C_ab = C_bc = 1, g = 1).
+  // only member a and b share, is left out of the walk when no heavy
+  // neighbour of a contains u: each c of the group closes a triangle
+  // {a, b, c} through u and shares only u with a as well (a heavy one would
+  // be in N+(a), ranked above b), so all are stars, counted by the size of c
+  // (lane 0 holds the group's counts).
   uint32_t gs = 0, glen = 0;
   if (!kTriads && T.skip && grouped && cab == 1) {
     const uint32_t qu = (uint32_t)(__ffsll((long long)mab) - 1);  // u's position in a (a has <= 64 members)
-    const uint32_t u = A.hmem[A.hoff[a] + qu];
-    const uint32_t* bm = A.hmem + A.hoff[b];
-    uint32_t lo = 0, hi = sb;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (bm[mid] < u) lo = mid + 1;
-      else hi = mid;
-    }
-    if (lo < kGroupPositions) {  // u's position in b; past 63 its entries sit in group 0 and are walked
-      const uint64_t t = A.wbase[b] + 1 + lo;
-      gs = A.wstart[t];
-      glen = A.wstart[t + 1] - gs;
+    const uint32_t pb = A.wopos[ao + bi];                        // u's position in b
+    if (!((T.heavy_or >> qu) & 1ull) && pb < kGroupPositions) {
+      const uint64_t t = A.wbase[b] + 1 + pb;
+      const uint4 g0 = A.wtab[t], g1 = A.wtab[t + 1];
+      gs = g0.x;
+      glen = g1.x - g0.x;
       if (lane == 0) {
-        star0 = A.wone[t];
-        star1 = A.wtwo[t];
-        star2 = glen - star0 - star1;
-      }
-      const uint32_t db = A.hdeg[b];
-      for (uint32_t k0 = 0; k0 < T.hv_n; k0 += kWarp) {
-        const uint32_t k = k0 + lane;
-        bool push = false;
-        uint64_t rec = 0;
-        if (k < T.hv_n) {
-          const uint64_t mac = T.hv_m[k];
-          const uint32_t c = T.hv_c[k];
-          if (((mac >> qu) & 1ull) && rank_above(b, db, c, A.hdeg[c])) {
-            const uint32_t sc = A.esize[c];
-            if (shared_upto2(bm, sb, A.hmem + A.hoff[c], sc) == 1) {  // b & c = {u}: in the skipped group
-              const uint32_t cc = size_cat(sc);
-              star0 -= cc == 0;  // per-lane counters summed modulo 2^32 below
-              star1 -= cc == 1;
-              star2 -= cc == 2;
-              push = true;
-              rec = pack_triangle(sb, sc, 1, 1, (uint32_t)__popcll(mac), 1);
-            }
-          }
-        }
-        queue_push(push, rec, q, qn, sa, wc);
+        star0 = g0.y;
+        star1 = g0.z;
+        star2 = glen - g0.y - g0.z;
       }
     }
   }
@@ -520,9 +465,8 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kHashSlotsMax);  // kHashSlotsMax
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];  // per warp: triangles waiting to be classified
-  __shared__ uint32_t hv_c[kHeavyBlock];
-  __shared__ uint64_t hv_m[kHeavyBlock];
-  __shared__ uint32_t s_item, hv_n;
+  __shared__ unsigned long long s_heavy;
+  __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long* wc = wcnt[w];
   uint64_t* q = wqueue[w];
@@ -533,7 +477,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   for (;;) {
     if (threadIdx.x == 0) {
       s_item = atomicAdd(A.queue, 1u);
-      hv_n = 0;
+      s_heavy = 0;
     }
     __syncthreads();
     const uint64_t item = (uint64_t)s_item * A.n_shards + A.shard;
@@ -550,7 +494,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const uint32_t ad = A.plen[a];
     const uint32_t sa = A.esize[a];
     const bool flags = A.edge_flags != nullptr;
-    CentreTable T{keys, sval, 32, 0, ad <= kHashRowMax, hv_c, hv_m, 0, false};
+    CentreTable T{keys, sval, 32, 0, ad <= kHashRowMax, 0, false};
     if (T.in_smem) {
       uint32_t slots = 64;
       while (slots < 4 * ad && slots < kHashSlotsMax) slots <<= 1;
@@ -559,14 +503,13 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x, hv_c, hv_m,
-                 &hv_n, kHeavyBlock);
+      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x, &s_heavy);
     }
     __syncthreads();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
-    T.hv_n = hv_n;
-    T.skip = T.in_smem && exact_masks && !flags && A.wnbr && T.hv_n <= kHeavyBlock;
+    T.heavy_or = s_heavy;
+    T.skip = T.in_smem && exact_masks && !flags && A.wnbr;
     for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
       closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
@@ -590,9 +533,7 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
   __shared__ uint64_t val_all[kClosedWarps][kWarpSlots];
   __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
   __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];
-  __shared__ uint32_t hvc_all[kClosedWarps][kHeavyWarp];
-  __shared__ uint64_t hvm_all[kClosedWarps][kHeavyWarp];
-  __shared__ uint32_t hvn_all[kClosedWarps];
+  __shared__ unsigned long long heavy_all[kClosedWarps];
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   uint32_t* keys = keys_all[w];
   uint64_t* sval = val_all[w];
@@ -623,18 +564,16 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     uint32_t slots = 64;
     while (slots < 2 * ad && slots < kWarpSlots) slots <<= 1;
     const uint32_t buckets = slots / 4;
-    CentreTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true, hvc_all[w], hvm_all[w], 0,
-                  false};
+    CentreTable T{keys, sval, 32u - (31u - (uint32_t)__clz(buckets)), buckets - 1, true, 0, false};
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
-    if (lane == 0) hvn_all[w] = 0;
+    if (lane == 0) heavy_all[w] = 0;
     __syncwarp();
-    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp, hvc_all[w], hvm_all[w],
-               &hvn_all[w], kHeavyWarp);
+    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp, &heavy_all[w]);
     __syncwarp();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
-    T.hv_n = hvn_all[w];
-    T.skip = exact_masks && !flags && A.wnbr && T.hv_n <= kHeavyWarp;
+    T.heavy_or = heavy_all[w];
+    T.skip = exact_masks && !flags && A.wnbr;
     for (uint32_t bi = 0; bi < ad; ++bi) {
       closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
@@ -763,10 +702,8 @@ static void with_groups(const hm_graph* g, ClosedArgs& A) {
   A.wnbr = g->grp_nbr.p;
   A.wos = g->grp_os.p;
   A.wbase = g->grp_base.p;
-  A.wstart = g->grp_start.p;
-  A.wone = g->grp_one.p;
-  A.wtwo = g->grp_two.p;
-  A.hdeg = g->h2h_len.p;
+  A.wtab = g->grp_tab.p;
+  A.wopos = g->grp_opos.p;
 }
 
 // Everything the count kernels need that only changes with the graph.
@@ -881,8 +818,8 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
       (uint64_t)g->plus_os.p,  (uint64_t)g->plus_mask.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
       (uint64_t)g->work.p,     (uint64_t)dev,            E,                       g->n_work,
       g->n_work_big,           g->n_work_mid,            shard,                   n_shards,
-      (uint64_t)args.wnbr,     (uint64_t)args.wos,       (uint64_t)args.wbase,    (uint64_t)args.wstart,
-      (uint64_t)args.wone,     (uint64_t)args.wtwo,      (uint64_t)args.hdeg};
+      (uint64_t)args.wnbr,     (uint64_t)args.wos,       (uint64_t)args.wbase,    (uint64_t)args.wtab,
+      (uint64_t)args.wopos,    0,                        0};
   CountCapture& C = g->capture;
   bool same = C.valid;
   for (unsigned k = 0; k < CountCapture::kKey && same; ++k) same = C.key[k] == key[k];

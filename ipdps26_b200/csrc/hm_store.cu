@@ -311,8 +311,8 @@ constexpr unsigned kGroupWarps = kBlock / kWarp;
 __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, const uint32_t* plen,
                                                        const uint32_t* pnbr, const uint16_t* pos,
                                                        const uint64_t* pmask, const uint8_t* esize, uint32_t n,
-                                                       const uint64_t* gbase, uint32_t* gstart, uint32_t* gone,
-                                                       uint32_t* gtwo, uint32_t* gnbr, uint16_t* gos) {
+                                                       const uint64_t* gbase, uint4* gtab, uint32_t* gnbr,
+                                                       uint16_t* gos) {
   __shared__ uint32_t cnt[kGroupWarps][kGroupPositions + 1];
   __shared__ uint32_t one[kGroupWarps][kGroupPositions + 1];
   __shared__ uint32_t two[kGroupWarps][kGroupPositions + 1];
@@ -337,14 +337,11 @@ __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, con
       uint32_t run = 0;
       for (uint32_t k = 0; k < G; ++k) {
         const uint32_t c = cnt[w][k];
-        gstart[t + k] = run;
-        gone[t + k] = one[w][k];
-        gtwo[t + k] = two[w][k];
+        gtab[t + k] = make_uint4(run, one[w][k], two[w][k], 0u);
         cnt[w][k] = run;  // becomes the group's write cursor
         run += c;
       }
-      gstart[t + G] = run;
-      gone[t + G] = gtwo[t + G] = 0;
+      gtab[t + G] = make_uint4(run, 0u, 0u, 0u);
     }
     __syncwarp();
     for (uint32_t i = lane; i < l; i += kWarp) {
@@ -354,6 +351,36 @@ __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, con
       gos[s + d] = o;
     }
     __syncwarp();
+  }
+}
+
+// One warp per row a: for each oriented entry (a, b) whose two hyperedges
+// share exactly one member u, at a position p < 64 of a, u's position in b
+// (a binary search of b's sorted members), 0xff for every other entry and
+// for a position of 64 or more in b.
+__global__ void k_shared_positions(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr,
+                                   const uint16_t* pos, const uint64_t* pmask, const uint64_t* hoff,
+                                   const uint32_t* hmem, const uint8_t* esize, uint32_t n, uint8_t* opos) {
+  for (uint64_t a = global_warp(); a < n; a += n_warps()) {
+    const uint64_t s = poff[a];
+    const uint32_t* am = hmem + hoff[a];
+    for (uint32_t i = lane_id(); i < plen[a]; i += kWarp) {
+      const uint64_t m = pmask[s + i];
+      uint8_t p = 0xff;
+      if ((pos[s + i] & 0xffu) == 1u && m) {
+        const uint32_t u = am[__ffsll((long long)m) - 1];
+        const uint32_t b = pnbr[s + i];
+        const uint32_t* bm = hmem + hoff[b];
+        uint32_t lo = 0, hi = esize[b];
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (bm[mid] < u) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo < kGroupPositions) p = (uint8_t)lo;
+      }
+      opos[s + i] = p;
+    }
   }
 }
 
@@ -375,15 +402,18 @@ int build_plus_groups(hm_graph* g) {
   uint64_t tab = 0;
   HM_CUDA(cudaMemcpyAsync(&tab, g->grp_base.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
-  HM_TRY(g->grp_start.alloc(ctx, tab));
-  HM_TRY(g->grp_one.alloc(ctx, tab));
-  HM_TRY(g->grp_two.alloc(ctx, tab));
+  HM_TRY(g->grp_tab.alloc(ctx, tab));
+  HM_TRY(g->grp_opos.alloc(ctx, g->plus_nnz));
   HM_TRY(g->grp_nbr.alloc(ctx, g->plus_nnz));
   HM_TRY(g->grp_os.alloc(ctx, g->plus_nnz));
   if (E) {
     k_group_rows<<<grid_for((uint64_t)E * kWarp, kBlock), kBlock, 0, st>>>(
         g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->esize.p, E, g->grp_base.p,
-        g->grp_start.p, g->grp_one.p, g->grp_two.p, g->grp_nbr.p, g->grp_os.p);
+        g->grp_tab.p, g->grp_nbr.p, g->grp_os.p);
+    HM_LAUNCH_CHECK();
+    k_shared_positions<<<grid_for((uint64_t)E * kWarp, kBlock), kBlock, 0, st>>>(
+        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p,
+        g->esize.p, E, g->grp_opos.p);
     HM_LAUNCH_CHECK();
   }
   g->grp_valid = true;
@@ -394,9 +424,8 @@ void release_plus_groups(hm_graph* g) {
   g->grp_nbr.release();
   g->grp_os.release();
   g->grp_base.release();
-  g->grp_start.release();
-  g->grp_one.release();
-  g->grp_two.release();
+  g->grp_tab.release();
+  g->grp_opos.release();
   g->grp_valid = false;
 }
 

@@ -91,6 +91,15 @@ FULL_CASES = {
         gen=dict(seed=3, n_nodes=200000, n_edges=500000, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2,
                  pop_offset=0.0, dedupe=False),
         burst=dict(burst_rate=1e-4, events_per_burst=50, gap_mean=20.0, span=100_000_000), deltas=[1000])),
+    # the same stream at the two wider windows of config 4
+    "config4-full-d10000": dict(kind="temporal", params=dict(
+        gen=dict(seed=3, n_nodes=200000, n_edges=500000, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2,
+                 pop_offset=0.0, dedupe=False),
+        burst=dict(burst_rate=1e-4, events_per_burst=50, gap_mean=20.0, span=100_000_000), deltas=[10000])),
+    "config4-full-d100000": dict(kind="temporal", params=dict(
+        gen=dict(seed=3, n_nodes=200000, n_edges=500000, k_min=2, k_max=20, size_exp=2.5, pop_exp=1.2,
+                 pop_offset=0.0, dedupe=False),
+        burst=dict(burst_rate=1e-4, events_per_burst=50, gap_mean=20.0, span=100_000_000), deltas=[100000])),
 }
 
 
