@@ -245,11 +245,13 @@ def update_section(args, g, p, counts30):
     log-uniform in [1000, 100000] edits, 80 % insertions drawn from the
     config-2 laws, 20 % deletions uniform over the live hyperedges (seed 2)."""
     from ipdps26_b200 import gen
+    from ipdps26_b200._lib import HmError
 
     rng = np.random.default_rng(2)
     total = counts30.astype(np.int64).copy()
     wall, dev, sizes, checks = [], [], [], []
     every = args.update_check_every
+    stopped = None
     for b in range(args.update_batches):
         n_edits = int(np.exp(rng.uniform(np.log(1_000), np.log(100_000))))
         if args.update_edits:
@@ -257,15 +259,31 @@ def update_section(args, g, p, counts30):
         live = g.live_ids()
         dels, ins = gen.batch(p, 2_000_000 + b, live, n_edits, 0.8)
         t0 = time.perf_counter()
-        _, delta = g.apply_batch(dels, ins.offsets, ins.members)
+        try:
+            _, delta = g.apply_batch(dels, ins.offsets, ins.members)
+        except HmError as err:
+            # a batch that fails part-way leaves the store unusable: the
+            # section ends here and says where and why
+            stopped = {"batch": b + 1, "edits": n_edits, "error": str(err),
+                       "device_gb_in_use": g.ctx.memory()[0] / 1e9}
+            print(f"[bench] update section stopped: {stopped}", file=sys.stderr, flush=True)
+            break
         wall.append(time.perf_counter() - t0)
         dev.append(g.timings().update_ms / 1000.0)
         sizes.append(n_edits)
         total += delta
         if every and ((b + 1) % every == 0 or b + 1 == args.update_batches):
-            full = g.count_static30().astype(np.int64)
+            try:
+                full = g.count_static30().astype(np.int64)
+            except HmError as err:
+                stopped = {"batch": b + 1, "in": "recount check", "error": str(err),
+                           "device_gb_in_use": g.ctx.memory()[0] / 1e9}
+                print(f"[bench] update section stopped: {stopped}", file=sys.stderr, flush=True)
+                break
             checks.append({"after_batch": b + 1, "equal": bool(np.array_equal(full, total))})
-    out = {"batches": len(wall), "edits_min": min(sizes), "edits_max": max(sizes),
+    if not wall:
+        return {"batches": 0, "stopped": stopped}
+    out = {"batches": len(wall), "stopped": stopped, "edits_min": min(sizes), "edits_max": max(sizes),
            "edits_total": int(sum(sizes)), "p50_ms": 1000 * pct(wall, 50), "p99_ms": 1000 * pct(wall, 99),
            "device_p50_ms": 1000 * pct(dev, 50), "device_p99_ms": 1000 * pct(dev, 99),
            "batches_per_s": len(wall) / sum(wall), "edits_per_s": sum(sizes) / sum(wall),
@@ -582,9 +600,12 @@ def engine_arm(args, rank, world, local_rank):
                    "h2d_bytes_per_step": int(off.nbytes + mem.nbytes), "d2h_bytes_per_step": 26 * 8,
                    "s_per_step": statistics.mean(times),
                    "note": "26 reported motifs; build of H2V/V2H/H2H included"}
+        mem_gb = {"after_static_and_e2e": ctx.memory()[0] / 1e9}
         base = None
         if world == 1 and not args.no_cpu_baseline:
             base = cpu_baseline(args, h, ctx)
+        mem_gb["before_updates"] = ctx.memory()[0] / 1e9
+        print(f"[bench] device memory in use: {mem_gb}", file=sys.stderr, flush=True)
         updates = None
         if args.update_batches > 0:
             updates = update_section(args, g, p, counts)
@@ -608,7 +629,7 @@ def engine_arm(args, rank, world, local_rank):
             "wall_s": wall, "clocks": clk.summary(), "roofline": roof, "e2e": e2e, "cpu_baseline": base,
             "graph": {"h2h_entries": int(info.n_adjacent), "oriented_entries": int(info.n_oriented),
                       "device_gb": info.device_bytes / 1e9},
-            "update_batches": updates, "temporal": temporal, "served": serve,
+            "update_batches": updates, "temporal": temporal, "served": serve, "device_memory_gb": mem_gb,
         }
         print(json.dumps(result), flush=True)
     g.close()

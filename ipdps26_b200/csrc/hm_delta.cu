@@ -32,7 +32,7 @@ constexpr unsigned kWarp = 32;
 constexpr unsigned kBlock = 256;
 constexpr unsigned kWarps = kBlock / kWarp;
 constexpr unsigned kSlots = 16384;        // shared table of one marked row (the longest rows): 192 KB
-constexpr unsigned kBigThreads = 512;     // its block: 16 warps, one block per SM
+constexpr unsigned kBigThreads = 1024;    // its block: 32 warps, one block per SM
 constexpr unsigned kRowMax = kSlots / 2;  // longer rows use a global table
 constexpr unsigned kMidSlots = 4096;      // rows up to mid_row <= kMidRow: 4096-slot tables, 4 blocks per SM
 constexpr unsigned kMidRow = kMidSlots / 2;
@@ -587,7 +587,7 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   for (size_t k = 0; k < (size_t)R * 30; ++k) out[k] = 0;
   if (!n) return HM_OK;
   const uint32_t E = g->n_slots;
-  const bool by_id = g->touch_by_id;
+  bool by_id = g->touch_by_id;
   const size_t n_cnt = (size_t)R * kRowStride + 5;  // + three queues, + class counts (u32 pairs)
   DArr<uint8_t> mark;
   DArr<uint32_t> flag, centres;
@@ -702,7 +702,18 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
     // the host copies above read pageable vectors: finish them before they go
     HM_CUDA(cudaStreamSynchronize(st));
   }
-  if (!by_id && !g->plus_valid) HM_TRY(build_plus(g));
+  if (!by_id && !g->plus_valid) {
+    // The oriented copy does not always fit beside a store that batches have
+    // grown: then this count walks the id-ordered row suffixes instead (the
+    // same triangles, met from their lower id rather than their lower rank).
+    const int s = build_plus(g);
+    if (s == HM_ERR_NOMEM) {
+      release_plus(g);
+      by_id = true;
+    } else {
+      HM_TRY(s);
+    }
+  }
   TouchArgs A{d_oid.p, n_items_long, sids.p + n_long, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
               g->h2h_ovl.p, g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p,
               g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,

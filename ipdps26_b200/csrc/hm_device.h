@@ -242,6 +242,7 @@ int h2h_rows_for(hm_graph* g, const uint32_t* d_rows, uint32_t n_rows,
 int build_plus(hm_graph* g);
 int build_plus_groups(hm_graph* g);
 void release_plus_groups(hm_graph* g);
+void release_plus(hm_graph* g);
 // Oriented rows of a subset of slots (indexed by slot; only listed slots valid).
 struct PlusRows {
   DArr<uint64_t> off;

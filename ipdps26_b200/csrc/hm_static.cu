@@ -713,7 +713,13 @@ int prepare_static(hm_graph* g) {
     HM_TRY(build_plus(g));
     g->work_valid = false;
   }
-  if (g->use_groups && !g->grp_valid) HM_TRY(build_plus_groups(g));
+  if (g->use_groups && !g->grp_valid) {
+    // the grouped rows are a shortcut: without room for them the count walks
+    // the oriented rows in full
+    const int s = build_plus_groups(g);
+    if (s == HM_ERR_NOMEM) release_plus_groups(g);
+    else HM_TRY(s);
+  }
   if (!g->work_valid && g->n_slots) HM_TRY(closed_worklist(g));
   if (!g->counters.p) HM_TRY(g->counters.alloc(ctx, 64));
   if (!g->ev_ready) {

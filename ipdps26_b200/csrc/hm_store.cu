@@ -420,6 +420,15 @@ int build_plus_groups(hm_graph* g) {
   return HM_OK;
 }
 
+// Frees the oriented copy (and the grouped one built from it).
+void release_plus(hm_graph* g) {
+  g->plus_nbr.release();
+  g->plus_os.release();
+  g->plus_mask.release();
+  g->plus_valid = false;
+  release_plus_groups(g);
+}
+
 void release_plus_groups(hm_graph* g) {
   g->grp_nbr.release();
   g->grp_os.release();

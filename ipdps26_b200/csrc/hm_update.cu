@@ -540,17 +540,19 @@ static int regrow_h2h(hm_graph* g, uint64_t cap) {
 // the live entries, dropping the oriented copy, which is rebuilt on demand),
 // then compacted in place whenever the tail runs out.
 static int compact_h2h(hm_graph* g, uint64_t extra) {
-  g->plus_nbr.release();
-  g->plus_os.release();
-  g->plus_mask.release();
-  g->plus_valid = false;
-  release_plus_groups(g);
+  release_plus(g);
   HM_TRY(compact_h2h_in_place(g));
   const uint64_t live = g->h2h_tail;
-  // keep at least half the live size free after a compaction, so that a
-  // batch needs few of them
+  // Keep at least half the live size free after a compaction, so that a
+  // batch needs few of them. A regrow holds the old and the new arena at
+  // once; when that does not fit the device budget, an arena that still has
+  // room for this request is kept (later batches compact more often), and
+  // one that has not is grown to the least that serves it.
   if (live + std::max<uint64_t>(extra, live / 2) <= g->h2h_cap) return HM_OK;
-  return regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
+  const int s = regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
+  if (s != HM_ERR_NOMEM) return s;
+  if (live + extra <= g->h2h_cap) return HM_OK;
+  return regrow_h2h(g, live + extra + (live + extra) / 16 + 1024);
 }
 
 // Grows the H2H arena to `factor` times the live entries (the first batch
@@ -669,6 +671,9 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
   HM_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
   if (hbad) return set_error(HM_ERR_NOT_LIVE, "apply_batch: a deleted id is not a live hyperedge");
+  // the static count's grouped rows die with this batch; their memory is
+  // better spent on the batch's own scratch
+  release_plus_groups(g);
 
   // normalised inserted member lists (sorted, unique) via a scratch graph
   hm_graph ins;
