@@ -280,7 +280,9 @@ def update_section(args, g, p, counts30):
                            "device_gb_in_use": g.ctx.memory()[0] / 1e9}
                 print(f"[bench] update section stopped: {stopped}", file=sys.stderr, flush=True)
                 break
-            checks.append({"after_batch": b + 1, "equal": bool(np.array_equal(full, total))})
+            checks.append({"after_batch": b + 1, "equal": bool(np.array_equal(full, total)),
+                           "recount_ms": round(g.timings().count_ms, 1),
+                           "h2h_entries": int(g.info().n_adjacent), "device_gb": g.ctx.memory()[0] / 1e9})
     if not wall:
         return {"batches": 0, "stopped": stopped}
     out = {"batches": len(wall), "stopped": stopped, "edits_min": min(sizes), "edits_max": max(sizes),
@@ -288,6 +290,7 @@ def update_section(args, g, p, counts30):
            "device_p50_ms": 1000 * pct(dev, 50), "device_p99_ms": 1000 * pct(dev, 99),
            "batches_per_s": len(wall) / sum(wall), "edits_per_s": sum(sizes) / sum(wall),
            "form": "plain per-call (hm_graph_apply_batch with the exact delta)",
+           "per_batch_ms": [round(1000 * w, 1) for w in wall], "per_batch_edits": sizes,
            "recount_checks": checks,
            "delta_sum_equals_full_recount": bool(checks) and all(c["equal"] for c in checks)}
     return out

@@ -12,8 +12,7 @@ std::atomic<long long> g_fail_after{-1};
 
 namespace hm {
 
-int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
-  *p = nullptr;
+int charge(hm_ctx* ctx, size_t bytes) {
   long long f = g_fail_after.load();
   if (f >= 0) {
     if (f == 0) return set_error(HM_ERR_NOMEM, "injected allocation failure (%zu bytes)", bytes);
@@ -23,6 +22,15 @@ int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
   if (ctx->budget && now + bytes > ctx->budget)
     return set_error(HM_ERR_NOMEM, "device budget exceeded: %zu used + %zu requested > %zu", now, bytes,
                      ctx->budget);
+  ctx->used.fetch_add(bytes);
+  return HM_OK;
+}
+
+void uncharge(hm_ctx* ctx, size_t bytes) { ctx->used.fetch_sub(bytes); }
+
+int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  HM_TRY(charge(ctx, bytes));
   // Stream-ordered allocation from the context's pool: no device-wide
   // synchronisation, and freed blocks are reused by the next call. When the
   // pool cannot grow, its cached free blocks are returned and the request is
@@ -37,9 +45,9 @@ int dev_alloc(hm_ctx* ctx, void** p, size_t bytes) {
   if (e != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
+    uncharge(ctx, bytes);
     return set_error(HM_ERR_NOMEM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
   }
-  ctx->used.fetch_add(bytes);
   return HM_OK;
 }
 

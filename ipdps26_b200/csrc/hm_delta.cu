@@ -167,7 +167,7 @@ struct TouchArgs {
   const uint32_t* plen;
   const uint32_t* pnbr;
   const uint16_t* pos;      // (neighbour size << 8) | overlap
-  const uint64_t* pmask;    // shared positions of the row owner's members
+  const uint32_t* prel;     // each oriented entry's index in its owner's H2H row
   const uint64_t* goff;     // per item: offset of its global table (rows longer than kRowMax)
   const uint32_t* gslots;   // per item: slots of that table, 0 for a shared-memory row
   const uint32_t* brange;   // per item: [brange[2i], brange[2i+1]) of row(m) to take b from
@@ -302,7 +302,6 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
     bl = A.plen[b];
   }
   const uint32_t* cnbr = A.by_id ? A.nbr : A.pnbr;
-  const uint64_t* cmask = A.by_id ? A.mask : A.pmask;
   // masks: relative to m when |m| <= 64, else relative to b when |b| <= 64
   const bool piv_m = sm <= 64, piv_b = !piv_m && sb <= 64;
   uint64_t pmb = piv_m ? A.mask[mo + bi] : 0;
@@ -369,7 +368,8 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
       const uint32_t cbc = ov[u] & 0xffu, sc = ov[u] >> 8;
       uint32_t g;
       if (piv_m || piv_b) {
-        const uint64_t pmc = piv_m ? mmc : cmask[bo + j0 + u * kWarp + lane];
+        const uint64_t jc = bo + j0 + u * kWarp + lane;
+        const uint64_t pmc = piv_m ? mmc : A.by_id ? A.mask[jc] : A.mask[A.off[b] + A.prel[jc]];
         if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
           const uint32_t cc = size_cat(sc);
           star0 += cc == 0;
@@ -716,7 +716,7 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   }
   TouchArgs A{d_oid.p, n_items_long, sids.p + n_long, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
               g->h2h_ovl.p, g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p,
-              g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
+              g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
               rows.gos, rows.rog, by_id, queues, cnt.p};
   if (trace) cudaStreamSynchronize(st);
   auto t_cl0 = std::chrono::steady_clock::now();

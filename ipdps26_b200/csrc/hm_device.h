@@ -81,6 +81,64 @@ struct DArr {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+int charge(hm_ctx* ctx, size_t bytes);  // budget only, no allocation
+void uncharge(hm_ctx* ctx, size_t bytes);
+bool vmm_available();  // the driver's virtual memory management calls were found
+
+// Device memory that grows without its contents moving: virtual address
+// space is reserved ahead and physical chunks are mapped at its end as it
+// grows (CUDA virtual memory management). When the reservation is full a
+// larger one is reserved and the chunks already held are mapped into it, so
+// growth never copies data and never holds two copies at once. Without VMM
+// support on the device it falls back to allocate-copy-free. Each grow and
+// release synchronises the device (chunks are unmapped only when no kernel
+// can use them). Budget-charged like DArr.
+struct GrowSpace {
+  hm_ctx* ctx = nullptr;
+  char* base = nullptr;
+  size_t mapped = 0;    // bytes usable from base
+  size_t reserved = 0;  // bytes of virtual address space at base
+  bool vmm = false;
+  std::vector<unsigned long long> handles;
+  std::vector<size_t> sizes;
+  int grow(hm_ctx* c, size_t bytes);  // mapped >= bytes afterwards, contents kept
+  void shrink(size_t bytes);          // gives back whole chunks past bytes (VMM only)
+  void release();
+  GrowSpace() = default;
+  GrowSpace(const GrowSpace&) = delete;
+  GrowSpace& operator=(const GrowSpace&) = delete;
+  ~GrowSpace() { release(); }
+};
+
+template <class T>
+struct GrowArr {
+  GrowSpace s;
+  T* p = nullptr;
+  size_t n = 0;  // entries usable
+  int alloc(hm_ctx* c, size_t count) {  // fresh, contents undefined
+    release();
+    return grow(c, count);
+  }
+  int grow(hm_ctx* c, size_t count) {  // keeps the first n entries
+    if (count == 0) count = 1;
+    if (count <= n) return 0;
+    HM_TRY(s.grow(c, count * sizeof(T)));
+    p = reinterpret_cast<T*>(s.base);
+    n = s.mapped / sizeof(T);
+    return 0;
+  }
+  void shrink(size_t count) {  // keeps at least the first count entries
+    s.shrink(count * sizeof(T));
+    n = s.mapped / sizeof(T);
+  }
+  void release() {
+    s.release();
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return s.mapped; }
+};
+
 // Per-phase device times of the last count call (CUDA events on the
 // context stream), reported through hm_graph_timings().
 struct PhaseTimes {
@@ -159,9 +217,10 @@ struct hm_graph {
 
   hm::DArr<uint64_t> h2h_off;
   hm::DArr<uint32_t> h2h_len;
-  hm::DArr<uint32_t> h2h_nbr;
-  hm::DArr<uint8_t> h2h_ovl;
-  hm::DArr<uint64_t> h2h_mask;
+  // the arena grows in place (a regrow compacts the rows, then maps more)
+  hm::GrowArr<uint32_t> h2h_nbr;
+  hm::GrowArr<uint8_t> h2h_ovl;
+  hm::GrowArr<uint64_t> h2h_mask;
   uint64_t h2h_tail = 0;
   uint64_t h2h_nnz = 0;  // live entries
   uint64_t h2h_cap = 0;  // arena entries allocated
@@ -175,7 +234,7 @@ struct hm_graph {
   hm::DArr<uint32_t> plus_len;
   hm::DArr<uint32_t> plus_nbr;
   hm::DArr<uint16_t> plus_os;  // (neighbour size << 8) | overlap
-  hm::DArr<uint64_t> plus_mask;
+  hm::DArr<uint32_t> plus_rel;  // each entry's index in its owner's H2H row (for the mask)
   uint64_t plus_nnz = 0;
   // The oriented rows once more, grouped for the static count's walk: in
   // each row, first the neighbours that share several members with the row
@@ -249,7 +308,7 @@ struct PlusRows {
   DArr<uint32_t> len;
   DArr<uint32_t> nbr;
   DArr<uint16_t> os;
-  DArr<uint64_t> mask;
+  DArr<uint32_t> rel;  // each entry's index in its owner's H2H row
   uint64_t nnz = 0;
 };
 int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P);
@@ -304,6 +363,7 @@ int apply_batch(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const uint6
 int modify_members(hm_graph* g, const uint32_t* h_ids, uint32_t n, const uint32_t* values, const uint64_t* prefix,
                    bool remove, int64_t* delta30);
 int presize_h2h(hm_graph* g, uint32_t factor);
+int trim_h2h(hm_graph* g);  // gives back the H2H arena's free tail
 
 // Orders the context stream's work after a caller's stream and the caller's
 // later work after it (two events); a null caller stream is CUDA's legacy

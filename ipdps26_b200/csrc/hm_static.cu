@@ -145,7 +145,7 @@ struct ClosedArgs {
   const uint32_t* plen;
   const uint32_t* pnbr;
   const uint16_t* pos;    // (neighbour size << 8) | overlap
-  const uint64_t* pmask;  // shared positions of the row owner's members (< 64)
+  const uint32_t* prel;   // each entry's index in its owner's H2H row
   const uint64_t* hoff;   // H2V
   const uint32_t* hmem;
   const uint8_t* esize;
@@ -165,6 +165,10 @@ struct ClosedArgs {
   const uint4* wtab;        // per group: {start in the row, size-1 neighbours, size-2 neighbours, 0}
   const uint8_t* wopos;     // per oriented entry (a, b), id-sorted: position in b of the one member
                             // a and b share, 0xff if they share several or it is past 63
+  // H2H offsets and shared-position masks (the row owner's members < 64),
+  // read through prel
+  const uint64_t* roff;
+  const uint64_t* rmask;
 };
 
 constexpr uint32_t kGroupPositions = 64;
@@ -236,7 +240,8 @@ struct CentreTable {
 // Fills the table with N+(a), threads t = first, first + stride, ...; the
 // masks of the entries sharing two or more members with a are ORed into
 // *heavy_or (when given).
-__device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uint32_t ad, uint32_t* keys,
+__device__ __forceinline__ void fill_table(const ClosedArgs& A, const uint64_t* amask, uint64_t ao, uint32_t ad,
+                                           uint32_t* keys,
                                            uint64_t* sval, uint32_t shift, uint32_t bmask, bool flags, bool exact,
                                            unsigned first, unsigned stride, unsigned long long* heavy_or) {
   for (uint32_t i = first; i < ad; i += stride) {
@@ -249,7 +254,7 @@ __device__ __forceinline__ void fill_table(const ClosedArgs& A, uint64_t ao, uin
           done = true;
           break;
         }
-    const uint64_t m = exact ? A.pmask[ao + i] : 0;
+    const uint64_t m = exact ? amask[A.prel[ao + i]] : 0;
     sval[h] = flags ? (uint64_t)i : exact ? m : (uint64_t)(A.pos[ao + i] & 0xffu);
     if (heavy_or && exact && (A.pos[ao + i] & 0xffu) >= 2u) atomicOr(heavy_or, (unsigned long long)m);
   }
@@ -292,7 +297,8 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   const uint32_t b = A.pnbr[ao + bi];
   const uint32_t osb = A.pos[ao + bi];
   const uint32_t cab = osb & 0xffu, sb = osb >> 8;
-  const uint64_t mab = A.pmask[ao + bi];
+  const uint64_t* amask = A.rmask + A.roff[a];
+  const uint64_t mab = amask[A.prel[ao + bi]];
   const uint64_t bo = A.poff[b];
   const uint32_t bd = A.plen[b];
   // N+(b) is walked in its grouped copy when there is one (any order of a
@@ -367,7 +373,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
             A.edge_flags[ao + bi] = 1;
             A.edge_flags[bo + j] = 1;
             cac = A.pos[ao + v] & 0xffu;
-            mac = A.pmask[ao + v];
+            mac = amask[A.prel[ao + v]];
           } else if (exact_masks) {
             mac = v;
             cac = (uint32_t)__popcll(v);
@@ -385,7 +391,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
         }
         if (lo < ad && row[lo] == c) {
           cac = A.pos[ao + lo] & 0xffu;
-          mac = A.pmask[ao + lo];
+          mac = amask[A.prel[ao + lo]];
           if (flags) {
             const uint32_t j = j0 + u * kWarp + lane;
             A.edge_flags[ao + lo] = 1;
@@ -503,7 +509,8 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x, blockDim.x, &s_heavy);
+      fill_table(A, A.rmask + A.roff[a], ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x,
+                 blockDim.x, &s_heavy);
     }
     __syncthreads();
     const uint32_t cat_a = size_cat(sa);
@@ -568,7 +575,8 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
     if (lane == 0) heavy_all[w] = 0;
     __syncwarp();
-    fill_table(A, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp, &heavy_all[w]);
+    fill_table(A, A.rmask + A.roff[a], ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp,
+               &heavy_all[w]);
     __syncwarp();
     const uint32_t cat_a = size_cat(sa);
     const bool exact_masks = sa <= 64;
@@ -697,7 +705,13 @@ static int prepare_static_attrs() {
 
 // The grouped rows and the rank the closed phase's walk uses (left null,
 // the walk takes the id-sorted rows and skips nothing).
+static void with_masks(const hm_graph* g, ClosedArgs& A) {
+  A.roff = g->h2h_off.p;
+  A.rmask = g->h2h_mask.p;
+}
+
 static void with_groups(const hm_graph* g, ClosedArgs& A) {
+  with_masks(g, A);
   if (!g->use_groups || !g->grp_valid) return;
   A.wnbr = g->grp_nbr.p;
   A.wos = g->grp_os.p;
@@ -792,7 +806,7 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p,
+  ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p,
                   g->h2v_off.p,  g->h2v_mem.p,  g->esize.p,    g->work.p,    0,
                   shard,         n_shards,      nullptr,       dev,          edge_flags,
                   nullptr,       nullptr};
@@ -821,11 +835,11 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   const uint64_t key[CountCapture::kKey] = {
       (uint64_t)g->h2h_off.p,  (uint64_t)g->h2h_len.p,  (uint64_t)g->h2h_nbr.p,   (uint64_t)g->h2h_ovl.p,
       (uint64_t)g->esize.p,    (uint64_t)g->plus_off.p, (uint64_t)g->plus_len.p,  (uint64_t)g->plus_nbr.p,
-      (uint64_t)g->plus_os.p,  (uint64_t)g->plus_mask.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
+      (uint64_t)g->plus_os.p,  (uint64_t)g->plus_rel.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
       (uint64_t)g->work.p,     (uint64_t)dev,            E,                       g->n_work,
       g->n_work_big,           g->n_work_mid,            shard,                   n_shards,
       (uint64_t)args.wnbr,     (uint64_t)args.wos,       (uint64_t)args.wbase,    (uint64_t)args.wtab,
-      (uint64_t)args.wopos,    0,                        0};
+      (uint64_t)args.wopos,    (uint64_t)g->h2h_mask.p,  0};
   CountCapture& C = g->capture;
   bool same = C.valid;
   for (unsigned k = 0; k < CountCapture::kKey && same; ++k) same = C.key[k] == key[k];
@@ -991,9 +1005,10 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   HM_CUDA(cudaStreamSynchronize(st));
   const uint32_t n_work = hw[0], n_big = hw[1];
   const uint32_t bounds[4] = {0, n_big, hw[2], n_work};
-  HM_TRY(launch_closed(ctx, ClosedArgs{P.off.p, P.len.p, P.nbr.p, P.os.p, P.mask.p, g->h2v_off.p, g->h2v_mem.p,
-                                       g->esize.p, work.p, 0, 0, 1, nullptr, cnt.p, nullptr, rows.gos, rows.rog},
-                       bounds, reinterpret_cast<unsigned int*>(tail)));
+  ClosedArgs pargs{P.off.p, P.len.p, P.nbr.p, P.os.p, P.rel.p, g->h2v_off.p, g->h2v_mem.p,
+                   g->esize.p, work.p, 0, 0, 1, nullptr, cnt.p, nullptr, rows.gos, rows.rog};
+  with_masks(g, pargs);
+  HM_TRY(launch_closed(ctx, pargs, bounds, reinterpret_cast<unsigned int*>(tail)));
   std::vector<unsigned long long> h((size_t)R * kRowStride);
   HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
@@ -1052,10 +1067,11 @@ int count_vertex_triads(hm_graph* g, uint64_t out3[3]) {
     HM_LAUNCH_CHECK();
   }
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  HM_TRY(launch_closed<true>(ctx, ClosedArgs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p,
-                                             g->plus_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->work.p, 0,
-                                             0, 1, nullptr, cnt.p, nullptr, nullptr, nullptr},
-                             bounds, reinterpret_cast<unsigned int*>(cnt.p + 1)));
+  ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2v_off.p,
+                   g->h2v_mem.p,    g->esize.p,    g->work.p,      0,             0,               1,
+                   nullptr,         cnt.p,         nullptr,        nullptr,       nullptr};
+  with_masks(g, targs);
+  HM_TRY(launch_closed<true>(ctx, targs, bounds, reinterpret_cast<unsigned int*>(cnt.p + 1)));
   unsigned long long h[8];
   HM_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
   HM_CUDA(cudaStreamSynchronize(st));
@@ -1171,7 +1187,7 @@ int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report& R) {
       HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
       HM_CUDA(cudaStreamSynchronize(st));
       const uint32_t bounds[4] = {0, hw[1], hw[2], hw[0]};
-      ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_mask.p, g->h2v_off.p,
+      ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2v_off.p,
                        g->h2v_mem.p,    g->esize.p,    work.p,         0,             0,               1,
                        nullptr,         cnt.p,         nullptr,        nullptr,       nullptr};
       with_groups(g, targs);

@@ -501,37 +501,22 @@ static int compact_h2h_in_place(hm_graph* g) {
   return HM_OK;
 }
 
-// Replaces the arena by one of cap entries holding the live rows compactly.
-static int regrow_h2h(hm_graph* g, uint64_t cap) {
+// Grows the arena to cap entries in place (more physical memory mapped after
+// the rows; nothing is copied and no second arena is held).
+static int grow_h2h(hm_graph* g, uint64_t cap) {
   hm_ctx* ctx = g->ctx;
-  cudaStream_t st = ctx->stream;
-  const uint32_t E = g->n_slots;
-  DArr<uint64_t> noff;
-  HM_TRY(noff.alloc(ctx, (size_t)E + 1));
-  HM_TRY(exclusive_scan(ctx, g->h2h_len.p, noff.p, E));
-  uint64_t live = 0;
-  HM_CUDA(cudaMemcpyAsync(&live, noff.p + E, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  HM_CUDA(cudaStreamSynchronize(st));
-  cap = std::max<uint64_t>(cap, live + 1024);
-  DArr<uint32_t> nnbr;
-  DArr<uint8_t> novl;
-  DArr<uint64_t> nmask;
-  HM_TRY(nnbr.alloc(ctx, cap));
-  HM_TRY(novl.alloc(ctx, cap));
-  HM_TRY(nmask.alloc(ctx, cap));
-  if (E) {
-    k_compact_rows<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, E, noff.p,
-                                                                        g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p,
-                                                                        nnbr.p, novl.p, nmask.p);
-    HM_LAUNCH_CHECK();
-    k_set_off<<<grid_for(E, kBlock), kBlock, 0, st>>>(noff.p, E, g->h2h_off.p);
-    HM_LAUNCH_CHECK();
-  }
-  g->h2h_nbr = static_cast<DArr<uint32_t>&&>(nnbr);
-  g->h2h_ovl = static_cast<DArr<uint8_t>&&>(novl);
-  g->h2h_mask = static_cast<DArr<uint64_t>&&>(nmask);
-  g->h2h_cap = cap;
-  g->h2h_tail = live;
+  cap = std::max<uint64_t>(cap, g->h2h_tail + 1024);
+  // all three arrays or none: a partial grow would hold memory the arena
+  // cannot use
+  auto more = [cap](size_t have, size_t width) { return cap > have ? (cap - have) * width : 0; };
+  const size_t bytes = more(g->h2h_nbr.n, 4) + more(g->h2h_ovl.n, 1) + more(g->h2h_mask.n, 8);
+  if (ctx->budget && ctx->used.load() + bytes + (8u << 20) > ctx->budget)
+    return set_error(HM_ERR_NOMEM, "H2H arena growth to %llu entries exceeds the device budget",
+                     (unsigned long long)cap);
+  HM_TRY(g->h2h_nbr.grow(ctx, cap));
+  HM_TRY(g->h2h_ovl.grow(ctx, cap));
+  HM_TRY(g->h2h_mask.grow(ctx, cap));
+  g->h2h_cap = std::min(std::min(g->h2h_nbr.n, g->h2h_ovl.n), g->h2h_mask.n);
   return HM_OK;
 }
 
@@ -540,19 +525,52 @@ static int regrow_h2h(hm_graph* g, uint64_t cap) {
 // the live entries, dropping the oriented copy, which is rebuilt on demand),
 // then compacted in place whenever the tail runs out.
 static int compact_h2h(hm_graph* g, uint64_t extra) {
+  hm_ctx* ctx = g->ctx;
   release_plus(g);
   HM_TRY(compact_h2h_in_place(g));
   const uint64_t live = g->h2h_tail;
   // Keep at least half the live size free after a compaction, so that a
-  // batch needs few of them. A regrow holds the old and the new arena at
-  // once; when that does not fit the device budget, an arena that still has
-  // room for this request is kept (later batches compact more often), and
-  // one that has not is grown to the least that serves it.
+  // batch needs few of them, but leave the device room for what the store
+  // needs besides the arena: the oriented copy of a count (10 bytes for
+  // each of about live / 2 entries) and a batch's scratch. Under that
+  // pressure the arena only grows to the least that serves this request
+  // (later batches compact more often).
   if (live + std::max<uint64_t>(extra, live / 2) <= g->h2h_cap) return HM_OK;
-  const int s = regrow_h2h(g, std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024);
-  if (s != HM_ERR_NOMEM) return s;
+  const uint64_t lean = live + extra + (live + extra) / 32 + 1024;
+  uint64_t want = std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024;
+  if (ctx->budget) {
+    const size_t arena = g->h2h_nbr.bytes() + g->h2h_ovl.bytes() + g->h2h_mask.bytes();
+    const size_t other = ctx->used.load() - std::min<size_t>(ctx->used.load(), arena);
+    const size_t reserve = (size_t)(live / 2) * 10 + (size_t(4) << 30);
+    const size_t room = ctx->budget > other + reserve ? ctx->budget - other - reserve : 0;
+    want = std::min<uint64_t>(want, room / 13);
+  }
+  const uint64_t keep = std::max(want, lean);
+  if (keep + (keep >> 4) < g->h2h_cap) {  // grown before the pressure: give the excess back
+    g->h2h_nbr.shrink(keep);
+    g->h2h_ovl.shrink(keep);
+    g->h2h_mask.shrink(keep);
+    g->h2h_cap = std::min(std::min(g->h2h_nbr.n, g->h2h_ovl.n), g->h2h_mask.n);
+  }
+  if (want <= g->h2h_cap && live + extra <= g->h2h_cap) return HM_OK;
+  const int s = grow_h2h(g, keep);
+  if (s != HM_ERR_NOMEM || want <= lean) return s;
   if (live + extra <= g->h2h_cap) return HM_OK;
-  return regrow_h2h(g, live + extra + (live + extra) / 16 + 1024);
+  return grow_h2h(g, lean);
+}
+
+// Gives the arena's free tail back to the device (compaction first), keeping
+// room for about 1/64 of the live entries; for callers about to allocate
+// under memory pressure.
+int trim_h2h(hm_graph* g) {
+  if (g->h2h_cap - g->h2h_nnz < (g->h2h_nnz >> 5) + (1u << 20)) return HM_OK;
+  HM_TRY(compact_h2h_in_place(g));
+  const uint64_t keep = g->h2h_tail + (g->h2h_tail >> 6) + 1024;
+  g->h2h_nbr.shrink(keep);
+  g->h2h_ovl.shrink(keep);
+  g->h2h_mask.shrink(keep);
+  g->h2h_cap = std::min(std::min(g->h2h_nbr.n, g->h2h_ovl.n), g->h2h_mask.n);
+  return HM_OK;
 }
 
 // Grows the H2H arena to `factor` times the live entries (the first batch
@@ -560,7 +578,9 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
 // pays for the growth up front.
 int presize_h2h(hm_graph* g, uint32_t factor) {
   const uint64_t want = (uint64_t)factor * g->h2h_nnz + 1024;
-  return g->h2h_cap < want ? regrow_h2h(g, want) : (int)HM_OK;
+  if (g->h2h_cap >= want) return HM_OK;
+  HM_TRY(compact_h2h_in_place(g));
+  return grow_h2h(g, want);
 }
 
 // Room for n more entries at the H2H arena tail; returns the position.
