@@ -47,8 +47,6 @@ namespace {
 constexpr unsigned kWarp = 32;
 constexpr unsigned kBlock = 256;
 constexpr unsigned kWarps = kBlock / kWarp;
-constexpr unsigned kSlots = 4096;       // neighbour hash slots
-constexpr unsigned kMaxNbrs = kSlots / 2; // neighbours of one event inside its window
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr uint32_t kNone = 0xffffffffu;
 
@@ -191,6 +189,9 @@ struct TArgs {
   // each event in its window, [1] adjacent pairs among them, [2] pairs
   // (b, c) with c adjacent to a neighbour b but not to the event
   unsigned long long* stats;
+  unsigned int* queue2;      // the deferred launch's queue
+  unsigned int* n_deferred;  // events set aside by the first launch
+  uint32_t* deferred;
 };
 
 // [first, last) of the sorted list x[0..n) restricted to values in [lo, hi)
@@ -249,38 +250,69 @@ __device__ __forceinline__ uint32_t overlap(const uint32_t* X, uint32_t nx, cons
   return c;
 }
 
-constexpr size_t kTemporalSmem = kSlots * (sizeof(unsigned long long) + 2 * sizeof(uint32_t)) + kMaxNbrs * sizeof(uint16_t);
+// Shared memory of one block: per neighbour (kM of them) its mask, first
+// window time, id, overlap with a, first window occurrence, occurrence count
+// and hash slot; the hash (kS keys, kS neighbour indices).
+template <uint32_t kS, uint32_t kM>
+constexpr size_t temporal_smem() {
+  return (size_t)kM * (2 * sizeof(unsigned long long) + 4 * sizeof(uint32_t) + sizeof(uint16_t)) +
+         (size_t)kS * (sizeof(uint32_t) + sizeof(uint16_t));
+}
 
+// Block per event; kS hash slots hold up to kM window neighbours. The first
+// launch (kFirst) takes every event and sets aside those with more
+// neighbours in a deferred list; the second takes that list with a larger
+// table, and reports an event that overflows it too.
+template <uint32_t kS, uint32_t kM, bool kFirst>
 __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
+  static_assert(kM <= 65535 && kS <= 65536 && (kS & (kS - 1)) == 0, "table shape");
+  constexpr uint32_t kHashShift = 32 - __builtin_ctz(kS);
   extern __shared__ unsigned long long tsm[];
-  unsigned long long* smask = tsm;                                     // kSlots
-  uint32_t* keys = reinterpret_cast<uint32_t*>(smask + kSlots);        // kSlots
-  uint32_t* scab = keys + kSlots;                                      // kSlots
-  uint16_t* la = reinterpret_cast<uint16_t*>(scab + kSlots);           // kMaxNbrs: slots of the neighbours
-  __shared__ unsigned long long cnt96[96];
+  unsigned long long* nmask = tsm;                                  // kM: a's member positions in b (< 64)
+  long long* nt0 = reinterpret_cast<long long*>(nmask + kM);        // kM: time of b's first window occurrence
+  uint32_t* nid = reinterpret_cast<uint32_t*>(nt0 + kM);            // kM: static id b
+  uint32_t* ncab = nid + kM;                                        // kM: C_ab
+  uint32_t* nof = ncab + kM;                                        // kM: first window occurrence (index into opos)
+  uint32_t* non = nof + kM;                                         // kM: window occurrences
+  uint32_t* keys = non + kM;                                        // kS
+  uint16_t* hidx = reinterpret_cast<uint16_t*>(keys + kS);          // kS: neighbour index of a slot
+  uint16_t* la = hidx + kS;                                         // kM: slot of a neighbour
+  __shared__ unsigned long long wcnt[kWarps][96];
+  __shared__ int8_t tab[128];
+  __shared__ uint32_t sam[256];
   __shared__ uint32_t s_item, s_nla;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
   unsigned long long n_nbrs = 0, n_closed = 0, n_open_b = 0;  // this thread's share of A.stats
-  for (unsigned k = threadIdx.x; k < 96; k += blockDim.x) cnt96[k] = 0;
+  for (unsigned k = threadIdx.x; k < kWarps * 96; k += blockDim.x) (&wcnt[0][0])[k] = 0;
+  for (unsigned k = threadIdx.x; k < 128; k += blockDim.x) tab[k] = c_temporal[k];
   // the table is cleared once here; after each event only the slots it used
   // are reset (all of them after an overflow)
-  for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
+  for (unsigned i = threadIdx.x; i < kS; i += blockDim.x) keys[i] = kEmpty;
+  auto tcls = [&](int s1, int s2, int s3, int c12, int c23, int c31, int g) {
+    return (int)tab[region_pattern(s1, s2, s3, c12, c23, c31, g)];
+  };
+  unsigned long long* wc = wcnt[w];
   for (;;) {
     if (threadIdx.x == 0) {
-      s_item = atomicAdd(A.queue, 1u);
+      s_item = atomicAdd(kFirst ? A.queue : A.queue2, 1u);
       s_nla = 0;
     }
     __syncthreads();
-    const uint32_t p = s_item;
-    if (p >= A.n) break;
+    const uint32_t item = s_item;
+    if (kFirst ? item >= A.n : item >= *A.n_deferred) break;
+    const uint32_t p = kFirst ? item : A.deferred[item];
     const uint32_t lo = A.lo[p];
     const uint32_t ea = A.order[p];
     const uint32_t sa = A.sp[p];
-    const uint32_t* am = A.hmem + A.hoff[ea];
     const uint32_t asz = A.hlen[ea];
-    // 1. neighbours of a in the window, overlap and member-position mask
+    const uint32_t* am = A.hmem + A.hoff[ea];
+    if (asz <= 256) {
+      for (uint32_t i = threadIdx.x; i < asz; i += blockDim.x) sam[i] = am[i];
+      am = sam;
+    }
+    // 1. neighbours of a in the window (first occurrence of each static id)
     for (uint32_t i = w; i < asz; i += kWarps) {
-      const uint32_t v = am[i];
+      const uint32_t v = A.hmem[A.hoff[ea] + i];
       const uint32_t* vp = A.vpos + A.voff[v];
       uint32_t f, l;
       range_in(vp, A.vlen[v], lo, p, f, l);
@@ -290,26 +322,41 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
         if (x == sa) continue;
         const uint32_t pr = A.prev[q];
         if (pr != kNone && pr >= lo) continue;  // not the first occurrence of x in the window
-        uint32_t h = (x * 2654435761u) >> (32 - 12);
+        uint32_t h = (x * 2654435761u) >> kHashShift;
         for (uint32_t probe = 0;; ++probe) {
-          if (probe == kSlots) {  // table full: more neighbours than the window limit
-            atomicAdd(&s_nla, (uint32_t)kSlots);
+          if (probe == kS) {  // table full: more neighbours than the window limit
+            atomicAdd(&s_nla, kS);
             break;
           }
           const uint32_t old = atomicCAS(&keys[h], kEmpty, x);
           if (old == kEmpty) {
             const uint32_t idx = atomicAdd(&s_nla, 1u);
-            if (idx < kMaxNbrs) la[idx] = (uint16_t)h;
-            scab[h] = 0;
-            smask[h] = 0;
+            if (idx < kM) {
+              hidx[h] = (uint16_t)idx;
+              la[idx] = (uint16_t)h;
+              nid[idx] = x;
+              ncab[idx] = 0;
+              nmask[idx] = 0;
+            }
           }
           if (old == kEmpty || old == x) break;
-          h = (h + 1) & (kSlots - 1);
+          h = (h + 1) & (kS - 1);
         }
       }
     }
     __syncthreads();
-    // counts are added in a second sweep so that initialisation precedes them
+    const uint32_t nla = s_nla;
+    if (nla > kM) {
+      if (threadIdx.x == 0) {
+        if (kFirst) A.deferred[atomicAdd(A.n_deferred, 1u)] = p;
+        else atomicExch(A.overflow, 1);
+      }
+      for (unsigned i = threadIdx.x; i < kS; i += blockDim.x) keys[i] = kEmpty;
+      __syncthreads();
+      continue;  // block-uniform
+    }
+    // overlaps and member positions (a second sweep, after initialisation),
+    // and each neighbour's window occurrences
     for (uint32_t i = w; i < asz; i += kWarps) {
       const uint32_t v = am[i];
       const uint32_t* vp = A.vpos + A.voff[v];
@@ -321,25 +368,23 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
         if (x == sa) continue;
         const uint32_t pr = A.prev[q];
         if (pr != kNone && pr >= lo) continue;
-        uint32_t h = (x * 2654435761u) >> (32 - 12);
-        uint32_t probe = 0;
-        while (keys[h] != x && probe < kSlots) {
-          h = (h + 1) & (kSlots - 1);
-          ++probe;
-        }
-        if (probe == kSlots) continue;  // not stored (overflow is reported)
-        atomicAdd(&scab[h], 1u);
-        if (i < 64) atomicOr(&smask[h], 1ull << i);
+        uint32_t h = (x * 2654435761u) >> kHashShift;
+        while (keys[h] != x) h = (h + 1) & (kS - 1);  // present: inserted above
+        const uint32_t idx = hidx[h];
+        atomicAdd(&ncab[idx], 1u);
+        if (i < 64) atomicOr(&nmask[idx], 1ull << i);
       }
     }
-    __syncthreads();
-    const uint32_t nla = s_nla;
-    if (nla > kMaxNbrs) {
-      if (threadIdx.x == 0) atomicExch(A.overflow, 1);
-      for (unsigned i = threadIdx.x; i < kSlots; i += blockDim.x) keys[i] = kEmpty;
-      __syncthreads();
-      continue;  // block-uniform; the whole count is reported as failed
+    for (uint32_t i = threadIdx.x; i < nla; i += blockDim.x) {
+      const uint32_t b = nid[i];
+      const uint32_t* bo = A.opos + A.ooff[b];
+      uint32_t bf, bl;
+      range_in(bo, A.olen[b], lo, p, bf, bl);
+      nof[i] = (uint32_t)A.ooff[b] + bf;
+      non[i] = bl - bf;
+      nt0[i] = A.tp[bo[bf]];  // bl > bf: b occurs in the window
     }
+    __syncthreads();
     if (threadIdx.x == 0) n_nbrs += nla;
     const uint32_t* ao = A.opos + A.ooff[sa];
     uint32_t af, al;
@@ -347,18 +392,15 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
     const uint32_t ta_n = al - af;
     // 2. pairs of neighbours
     for (uint32_t i = w; i < nla; i += kWarps) {
-      const uint32_t hb = la[i];
-      const uint32_t b = keys[hb], cab = scab[hb];
-      const unsigned long long mb = smask[hb];
+      const uint32_t b = nid[i], cab = ncab[i];
+      const unsigned long long mb = nmask[i];
       const uint32_t* bm = A.hmem + A.hoff[b];
       const uint32_t bsz = A.hlen[b];
-      const uint32_t* bo = A.opos + A.ooff[b];
-      uint32_t bf, bl;
-      range_in(bo, A.olen[b], lo, p, bf, bl);
+      const uint32_t bn = non[i];
+      const uint32_t* bo = A.opos + nof[i];
+      const long long tb = nt0[i];
       for (uint32_t j = i + 1 + lane; j < nla; j += kWarp) {
-        const uint32_t hc = la[j];
-        const uint32_t c = keys[hc], cac = scab[hc];
-        const unsigned long long mc = smask[hc];
+        const uint32_t c = nid[j], cac = ncab[j];
         const uint32_t* cm = A.hmem + A.hoff[c];
         const uint32_t csz = A.hlen[c];
         uint32_t first;
@@ -367,7 +409,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
         n_closed += cbc != 0;
         if (cbc) {
           if (asz <= 64) {
-            g = __popcll(mb & mc);
+            g = __popcll(mb & nmask[j]);
           } else {
             // |a & b & c| by merging a's members with the b & c shared list
             uint32_t x = 0, y = 0, z = 0;
@@ -379,44 +421,44 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
             }
           }
         }
-        const uint32_t* co = A.opos + A.ooff[c];
-        uint32_t cf, cl;
-        range_in(co, A.olen[c], lo, p, cf, cl);
-        const uint32_t nb = bl - bf, nc = cl - cf;
+        const uint32_t cn = non[j];
         // Of the two, the node-set that comes first in the input (the smaller
         // static id) plays THyMe's "b": occurrence pairs with it strictly
         // earlier go to its order, all others (ties too) to the other order.
-        const uint64_t bc = b < c ? ordered_pairs(A.tp, bo + bf, nb, co + cf, nc)
-                                  : (uint64_t)nb * nc - ordered_pairs(A.tp, co + cf, nc, bo + bf, nb);
-        const uint64_t cb = (uint64_t)nb * nc - bc;
-        const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, (int)cac, (int)cab, (int)g);
-        const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, (int)cac, (int)g);
-        if (bc && kbc >= 0) atomicAdd(&cnt96[kbc], (unsigned long long)bc);
-        if (cb && kcb >= 0) atomicAdd(&cnt96[kcb], (unsigned long long)cb);
+        uint64_t bc;
+        if (bn == 1 && cn == 1) {
+          const long long tc = nt0[j];
+          bc = b < c ? tb < tc : tb <= tc;
+        } else {
+          const uint32_t* co = A.opos + nof[j];
+          bc = b < c ? ordered_pairs(A.tp, bo, bn, co, cn) : (uint64_t)bn * cn - ordered_pairs(A.tp, co, cn, bo, bn);
+        }
+        const uint64_t cb = (uint64_t)bn * cn - bc;
+        const int kbc = tcls((int)bsz, (int)csz, (int)asz, (int)cbc, (int)cac, (int)cab, (int)g);
+        const int kcb = tcls((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, (int)cac, (int)g);
+        if (bc && kbc >= 0) atomicAdd(&wc[kbc], (unsigned long long)bc);
+        if (cb && kcb >= 0) atomicAdd(&wc[kcb], (unsigned long long)cb);
       }
       // 4. motifs 87-95 for the pair (a, b)
       if (lane == 0) {
-        const uint32_t tb_n = bl - bf;
-        const uint64_t ab = ordered_pairs(A.tp, ao + af, ta_n, bo + bf, tb_n);
-        const uint64_t ba = (uint64_t)ta_n * tb_n - ab;
-        const uint64_t bb = (uint64_t)tb_n * (tb_n ? tb_n - 1 : 0) / 2;
-        const int kab = tclass((int)asz, (int)bsz, (int)asz, (int)cab, (int)cab, (int)asz, (int)cab);
-        const int kba = tclass((int)bsz, (int)asz, (int)asz, (int)cab, (int)asz, (int)cab, (int)cab);
-        const int kbb = tclass((int)bsz, (int)bsz, (int)asz, (int)bsz, (int)cab, (int)cab, (int)cab);
-        if (ab && kab >= 0) atomicAdd(&cnt96[kab], (unsigned long long)ab);
-        if (ba && kba >= 0) atomicAdd(&cnt96[kba], (unsigned long long)ba);
-        if (bb && kbb >= 0) atomicAdd(&cnt96[kbb], (unsigned long long)bb);
+        const uint64_t ab = ordered_pairs(A.tp, ao + af, ta_n, bo, bn);
+        const uint64_t ba = (uint64_t)ta_n * bn - ab;
+        const uint64_t bb = (uint64_t)bn * (bn ? bn - 1 : 0) / 2;
+        const int kab = tcls((int)asz, (int)bsz, (int)asz, (int)cab, (int)cab, (int)asz, (int)cab);
+        const int kba = tcls((int)bsz, (int)asz, (int)asz, (int)cab, (int)asz, (int)cab, (int)cab);
+        const int kbb = tcls((int)bsz, (int)bsz, (int)asz, (int)bsz, (int)cab, (int)cab, (int)cab);
+        if (ab && kab >= 0) atomicAdd(&wc[kab], (unsigned long long)ab);
+        if (ba && kba >= 0) atomicAdd(&wc[kba], (unsigned long long)ba);
+        if (bb && kbb >= 0) atomicAdd(&wc[kbb], (unsigned long long)bb);
       }
     }
     // 3. open at b: c meets b outside a and misses a
     for (uint32_t i = w; i < nla; i += kWarps) {
-      const uint32_t hb = la[i];
-      const uint32_t b = keys[hb], cab = scab[hb];
+      const uint32_t b = nid[i], cab = ncab[i];
       const uint32_t* bm = A.hmem + A.hoff[b];
       const uint32_t bsz = A.hlen[b];
-      const uint32_t* bo = A.opos + A.ooff[b];
-      uint32_t bf, bl;
-      range_in(bo, A.olen[b], lo, p, bf, bl);
+      const uint32_t bn = non[i];
+      const uint32_t* bo = A.opos + nof[i];
       for (uint32_t kk = 0; kk < bsz; ++kk) {
         const uint32_t v = bm[kk];
         // skip nodes of a (a's members are sorted)
@@ -437,13 +479,13 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
           const uint32_t pr = A.prev[q];
           if (pr != kNone && pr >= lo) continue;
           // c must miss a: not a neighbour of a
-          uint32_t h = (c * 2654435761u) >> (32 - 12);
+          uint32_t h = (c * 2654435761u) >> kHashShift;
           bool nbr_of_a = false;
           for (;;) {
             const uint32_t kh = keys[h];
             if (kh == c) { nbr_of_a = true; break; }
             if (kh == kEmpty) break;
-            h = (h + 1) & (kSlots - 1);
+            h = (h + 1) & (kS - 1);
           }
           if (nbr_of_a) continue;
           const uint32_t* cm = A.hmem + A.hoff[c];
@@ -455,24 +497,27 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
           const uint32_t* co = A.opos + A.ooff[c];
           uint32_t cf, cl;
           range_in(co, A.olen[c], lo, p, cf, cl);
-          const uint32_t nb = bl - bf, nc = cl - cf;
-          const uint64_t bc = ordered_pairs(A.tp, bo + bf, nb, co + cf, nc);
-          const uint64_t cb = (uint64_t)nb * nc - bc;
-          const int kbc = tclass((int)bsz, (int)csz, (int)asz, (int)cbc, 0, (int)cab, 0);
-          const int kcb = tclass((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, 0, 0);
-          if (bc && kbc >= 0) atomicAdd(&cnt96[kbc], (unsigned long long)bc);
-          if (cb && kcb >= 0) atomicAdd(&cnt96[kcb], (unsigned long long)cb);
+          const uint32_t nc = cl - cf;
+          const uint64_t bc = ordered_pairs(A.tp, bo, bn, co + cf, nc);
+          const uint64_t cb = (uint64_t)bn * nc - bc;
+          const int kbc = tcls((int)bsz, (int)csz, (int)asz, (int)cbc, 0, (int)cab, 0);
+          const int kcb = tcls((int)csz, (int)bsz, (int)asz, (int)cbc, (int)cab, 0, 0);
+          if (bc && kbc >= 0) atomicAdd(&wc[kbc], (unsigned long long)bc);
+          if (cb && kcb >= 0) atomicAdd(&wc[kcb], (unsigned long long)cb);
         }
       }
     }
     // 4. motif 96: two earlier occurrences of a
-    if (threadIdx.x == 0 && ta_n >= 2) atomicAdd(&cnt96[95], (unsigned long long)ta_n * (ta_n - 1) / 2);
+    if (threadIdx.x == 0 && ta_n >= 2) atomicAdd(&wc[95], (unsigned long long)ta_n * (ta_n - 1) / 2);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < nla; i += blockDim.x) keys[la[i]] = kEmpty;  // reset the used slots
   }
   __syncthreads();
-  for (unsigned k = threadIdx.x; k < 96; k += blockDim.x)
-    if (cnt96[k]) atomicAdd(&A.out[k], cnt96[k]);
+  for (unsigned k = threadIdx.x; k < 96; k += blockDim.x) {
+    unsigned long long t = 0;
+    for (unsigned ww = 0; ww < kWarps; ++ww) t += wcnt[ww][k];
+    if (t) atomicAdd(&A.out[k], t);
+  }
   for (int d = 16; d; d >>= 1) {
     n_nbrs += __shfl_xor_sync(0xffffffffu, n_nbrs, d);
     n_closed += __shfl_xor_sync(0xffffffffu, n_closed, d);
@@ -484,6 +529,11 @@ __global__ void __launch_bounds__(kBlock) k_temporal(TArgs A) {
     if (n_open_b) atomicAdd(&A.stats[2], n_open_b);
   }
 }
+
+// Table shapes: the first launch's (4 blocks per SM) and the deferred one's.
+constexpr uint32_t kSlotsSmall = 2048, kNbrsSmall = 1024;
+constexpr uint32_t kSlotsLarge = 8192, kNbrsLarge = 4096;
+constexpr uint32_t kMaxNbrs = kNbrsLarge;  // neighbours of one event inside its window
 
 template <class K, class V>
 int sort_pairs(hm_ctx* ctx, const K* kin, K* kout, const V* vin, V* vout, uint64_t n, int end_bit) {
@@ -602,30 +652,59 @@ __global__ void k_temporal_finish(const unsigned long long* acc, uint64_t* out96
 }
 }  // namespace
 
-// Queues the window starts and the counting kernel on the context stream:
+// Queues the window starts and the counting kernels on the context stream:
 // acc receives the 96 counts, [96] the work queue, [97] the overflow flag,
-// [98..100] the window-projection sizes. Events e0/e1 bracket the kernels.
+// [98..100] the window-projection sizes, [101] the deferred launch's queue,
+// [102] the number of deferred events; lo holds the window starts and then
+// the deferred events. Events e0/e1 bracket the kernels.
 static int launch_temporal(hm_graph* g, int64_t delta, DArr<uint32_t>& lo, DArr<unsigned long long>& acc,
                            cudaEvent_t e0, cudaEvent_t e1) {
   hm_ctx* ctx = g->ctx;
   cudaStream_t st = ctx->stream;
   const uint32_t n = g->n_slots;
   if (!g->t_ready) HM_TRY(build_temporal_index(g));
-  HM_TRY(lo.alloc(ctx, n));
-  HM_TRY(acc.alloc(ctx, 101));
-  HM_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 101, st));
+  HM_TRY(lo.alloc(ctx, 2 * (size_t)n));
+  HM_TRY(acc.alloc(ctx, 103));
+  HM_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 103, st));
   if (e0) HM_CUDA(cudaEventRecord(e0, st));
   k_window_lo<<<grid_for(n, kBlock), kBlock, 0, st>>>(g->t_time.p, n, delta, lo.p);
   HM_LAUNCH_CHECK();
-  TArgs A{n, g->t_order.p, g->t_static.p, g->t_prev.p, lo.p, g->h2v_off.p, g->h2v_len.p, g->h2v_mem.p,
-          g->t_voff.p, g->t_vlen.p, g->t_vpos.p, g->t_ooff.p, g->t_olen.p, g->t_opos.p, g->t_time.p,
-          reinterpret_cast<unsigned int*>(acc.p + 96), acc.p, reinterpret_cast<int*>(acc.p + 97), acc.p + 98};
+  TArgs A{n,
+          g->t_order.p,
+          g->t_static.p,
+          g->t_prev.p,
+          lo.p,
+          g->h2v_off.p,
+          g->h2v_len.p,
+          g->h2v_mem.p,
+          g->t_voff.p,
+          g->t_vlen.p,
+          g->t_vpos.p,
+          g->t_ooff.p,
+          g->t_olen.p,
+          g->t_opos.p,
+          g->t_time.p,
+          reinterpret_cast<unsigned int*>(acc.p + 96),
+          acc.p,
+          reinterpret_cast<int*>(acc.p + 97),
+          acc.p + 98,
+          reinterpret_cast<unsigned int*>(acc.p + 101),
+          reinterpret_cast<unsigned int*>(acc.p + 102),
+          lo.p + n};
+  constexpr size_t kSmemSmall = temporal_smem<kSlotsSmall, kNbrsSmall>();
+  constexpr size_t kSmemLarge = temporal_smem<kSlotsLarge, kNbrsLarge>();
   static bool attr = false;
   if (!attr) {
-    HM_CUDA(cudaFuncSetAttribute(k_temporal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTemporalSmem));
+    HM_CUDA(cudaFuncSetAttribute(k_temporal<kSlotsSmall, kNbrsSmall, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemSmall));
+    HM_CUDA(cudaFuncSetAttribute(k_temporal<kSlotsLarge, kNbrsLarge, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLarge));
     attr = true;
   }
-  k_temporal<<<std::min<unsigned>((unsigned)ctx->n_sms * 3, n), kBlock, kTemporalSmem, st>>>(A);
+  k_temporal<kSlotsSmall, kNbrsSmall, true>
+      <<<std::min<unsigned>((unsigned)ctx->n_sms * 4, n), kBlock, kSmemSmall, st>>>(A);
+  HM_LAUNCH_CHECK();
+  k_temporal<kSlotsLarge, kNbrsLarge, false><<<(unsigned)ctx->n_sms, kBlock, kSmemLarge, st>>>(A);
   HM_LAUNCH_CHECK();
   if (e1) HM_CUDA(cudaEventRecord(e1, st));
   return HM_OK;
@@ -650,7 +729,7 @@ int count_temporal96(hm_graph* g, int64_t delta, uint64_t out96[96]) {
   HM_CUDA(cudaEventCreate(&e0));
   HM_CUDA(cudaEventCreate(&e1));
   const int rc = launch_temporal(g, delta, lo, acc, e0, e1);
-  unsigned long long h[101];
+  unsigned long long h[103];
   cudaError_t ce = rc < 0 ? cudaSuccess : cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, st);
   if (rc >= 0 && ce == cudaSuccess) ce = cudaStreamSynchronize(st);
   float ms = 0;

@@ -520,28 +520,28 @@ static int grow_h2h(hm_graph* g, uint64_t cap) {
   return HM_OK;
 }
 
-// The arena keeps room for rewriting about as many entries as are live: a
-// batch on a hub-heavy graph rewrites most rows. It is grown once (to twice
-// the live entries, dropping the oriented copy, which is rebuilt on demand),
-// then compacted in place whenever the tail runs out.
+// Called when the arena tail runs out: drops the oriented copy (rebuilt on
+// demand), compacts in place, and grows the arena in place when the live
+// rows leave too little room (a batch on a hub-heavy graph rewrites most
+// rows, in chunks that each need free tail).
 static int compact_h2h(hm_graph* g, uint64_t extra) {
   hm_ctx* ctx = g->ctx;
   release_plus(g);
   HM_TRY(compact_h2h_in_place(g));
   const uint64_t live = g->h2h_tail;
-  // Keep at least half the live size free after a compaction, so that a
-  // batch needs few of them, but leave the device room for what the store
+  // Keep about half the live size free after a compaction, so that a batch
+  // needs few of them, but leave the device room for what the store
   // needs besides the arena: the oriented copy of a count (10 bytes for
   // each of about live / 2 entries) and a batch's scratch. Under that
   // pressure the arena only grows to the least that serves this request
   // (later batches compact more often).
   if (live + std::max<uint64_t>(extra, live / 2) <= g->h2h_cap) return HM_OK;
   const uint64_t lean = live + extra + (live + extra) / 32 + 1024;
-  uint64_t want = std::max<uint64_t>(2 * live, live + extra + (live + extra) / 8) + 1024;
+  uint64_t want = std::max<uint64_t>(live + live / 2, live + extra + (live + extra) / 8) + 1024;
   if (ctx->budget) {
     const size_t arena = g->h2h_nbr.bytes() + g->h2h_ovl.bytes() + g->h2h_mask.bytes();
     const size_t other = ctx->used.load() - std::min<size_t>(ctx->used.load(), arena);
-    const size_t reserve = (size_t)(live / 2) * 10 + (size_t(4) << 30);
+    const size_t reserve = (size_t)(live / 2) * 10 + (size_t(8) << 30);
     const size_t room = ctx->budget > other + reserve ? ctx->budget - other - reserve : 0;
     want = std::min<uint64_t>(want, room / 13);
   }

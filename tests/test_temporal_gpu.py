@@ -110,3 +110,46 @@ def test_temporal_with_equal_times_matches_oracle(ctx, seed):
             for delta in (0, 1, 3, 10):
                 want = oracle.temporal96(off, mem, times, delta)
                 assert g.count_temporal(delta).tolist() == want.tolist(), (rows, times.tolist(), delta)
+
+
+def spokes_and_centres(rng, nodes_per_centre, spokes_per_node, centres):
+    """Small "spoke" events {v, unique node} and, after them, large "centre"
+    events over the spokes' shared nodes: a centre's window holds about
+    nodes_per_centre * spokes_per_node neighbours while the spokes' own
+    windows stay small."""
+    n_shared = nodes_per_centre + 20 * (centres - 1)
+    spokes = [[v, 100_000 + j] for j, v in enumerate(rng.permutation(np.repeat(np.arange(1, n_shared + 1),
+                                                                                   spokes_per_node)))]
+    cents = [list(range(1 + 20 * c, 1 + 20 * c + nodes_per_centre)) for c in range(centres)]
+    rows = spokes + cents
+    off, mem = csr(rows)
+    times = np.arange(len(rows), dtype=np.int64)
+    return off, mem, times, 100_000 + len(spokes)
+
+
+def test_temporal_wide_windows_take_the_deferred_launch(ctx):
+    """Events with more than 1,024 window neighbours are set aside by the first
+    launch and counted by the second (8,192-slot table): centres with about
+    1,200 neighbours, against the oracle."""
+    from ipdps26_b200 import engine
+
+    rng = np.random.default_rng(77)
+    off, mem, times, n_nodes = spokes_and_centres(rng, 100, 12, 3)
+    with engine.Graph(ctx, off, mem, n_nodes, times) as g:
+        got = g.count_temporal(1_000_000)
+    assert got.tolist() == oracle.temporal96(off, mem, times, 1_000_000).tolist()
+
+
+def test_temporal_window_limit_is_an_error(ctx):
+    """More than 4,096 neighbours of one event inside its window is reported
+    (HM_ERR_LIMIT), not counted wrong, and the graph stays usable."""
+    from ipdps26_b200 import engine
+    from ipdps26_b200._lib import HM_ERR_LIMIT, HmError
+
+    rng = np.random.default_rng(78)
+    off, mem, times, n_nodes = spokes_and_centres(rng, 250, 17, 1)
+    with engine.Graph(ctx, off, mem, n_nodes, times) as g:
+        with pytest.raises(HmError) as e:
+            g.count_temporal(1_000_000)
+        assert e.value.status == HM_ERR_LIMIT
+        assert g.count_temporal(10).tolist() == oracle.temporal96(off, mem, times, 10).tolist()
