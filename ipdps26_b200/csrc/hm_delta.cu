@@ -167,7 +167,6 @@ struct TouchArgs {
   const uint32_t* plen;
   const uint32_t* pnbr;
   const uint16_t* pos;      // (neighbour size << 8) | overlap
-  const uint32_t* prel;     // each oriented entry's index in its owner's H2H row
   const uint64_t* goff;     // per item: offset of its global table (rows longer than kRowMax)
   const uint32_t* gslots;   // per item: slots of that table, 0 for a shared-memory row
   const uint32_t* brange;   // per item: [brange[2i], brange[2i+1]) of row(m) to take b from
@@ -311,21 +310,35 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
   }
   const bool star_ok = cmb == 1 && (piv_m || piv_b);
   uint32_t star0 = 0, star1 = 0, star2 = 0;
+  // The next round's loads are issued before this round's probes (software
+  // pipelining); by id, a neighbour's size is gathered when it is probed.
+  uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+  for (unsigned u = 0; u < kUnroll; ++u) {
+    const uint32_t j = u * kWarp + lane;
+    cv[u] = kEmpty;
+    ov[u] = 0;
+    if (j < bl) {
+      cv[u] = __ldg(cnbr + bo + j);
+      ov[u] = A.by_id ? __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
+    }
+  }
   for (uint32_t j0 = 0; j0 < bl; j0 += kWarp * kUnroll) {
-    uint32_t cv[kUnroll], ov[kUnroll];
+    uint32_t cn[kUnroll], on[kUnroll];
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
-      const uint32_t j = j0 + u * kWarp + lane;
-      cv[u] = kEmpty;
-      ov[u] = 0;
+      const uint32_t j = j0 + kWarp * kUnroll + u * kWarp + lane;
+      cn[u] = kEmpty;
+      on[u] = 0;
       if (j < bl) {
-        cv[u] = __ldg(cnbr + bo + j);
-        ov[u] = A.by_id ? ((uint32_t)__ldg(A.esize + cv[u]) << 8) | __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
+        cn[u] = __ldg(cnbr + bo + j);
+        on[u] = A.by_id ? __ldg(A.ovl + bo + j) : __ldg(A.pos + bo + j);
       }
     }
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
       const uint32_t c = cv[u];
+      if (A.by_id && c != kEmpty) ov[u] |= (uint32_t)__ldg(A.esize + c) << 8;
       bool push = false;
       uint64_t rec = 0;
       do {
@@ -369,7 +382,7 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
       uint32_t g;
       if (piv_m || piv_b) {
         const uint64_t jc = bo + j0 + u * kWarp + lane;
-        const uint64_t pmc = piv_m ? mmc : A.by_id ? A.mask[jc] : A.mask[A.off[b] + A.prel[jc]];
+        const uint64_t pmc = piv_m ? mmc : A.by_id ? A.mask[jc] : row_mask(A.off, A.len, A.nbr, A.mask, b, c);
         if ((cmb | cmc | cbc) == 1 && pmb == pmc) {
           const uint32_t cc = size_cat(sc);
           star0 += cc == 0;
@@ -395,6 +408,11 @@ __device__ __forceinline__ void touch_pairs_of_b(const TouchArgs& A, uint32_t m,
         __syncwarp();
         qn -= kWarp;
       }
+    }
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      cv[u] = cn[u];
+      ov[u] = on[u];
     }
   }
   if (star_ok) {
@@ -716,7 +734,7 @@ int count_touching_rows(hm_graph* g, const uint32_t* d_ids, uint32_t n, const To
   }
   TouchArgs A{d_oid.p, n_items_long, sids.p + n_long, n_items, mark.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
               g->h2h_ovl.p, g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, g->plus_off.p, g->plus_len.p,
-              g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
+              g->plus_nbr.p, g->plus_os.p, d_ooff.p, d_oslots.p, d_orange.p, gtab.p,
               rows.gos, rows.rog, by_id, queues, cnt.p};
   if (trace) cudaStreamSynchronize(st);
   auto t_cl0 = std::chrono::steady_clock::now();

@@ -234,7 +234,6 @@ struct hm_graph {
   hm::DArr<uint32_t> plus_len;
   hm::DArr<uint32_t> plus_nbr;
   hm::DArr<uint16_t> plus_os;  // (neighbour size << 8) | overlap
-  hm::DArr<uint32_t> plus_rel;  // each entry's index in its owner's H2H row (for the mask)
   uint64_t plus_nnz = 0;
   // The oriented rows once more, grouped for the static count's walk: in
   // each row, first the neighbours that share several members with the row
@@ -308,7 +307,6 @@ struct PlusRows {
   DArr<uint32_t> len;
   DArr<uint32_t> nbr;
   DArr<uint16_t> os;
-  DArr<uint32_t> rel;  // each entry's index in its owner's H2H row
   uint64_t nnz = 0;
 };
 int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P);
@@ -409,6 +407,21 @@ struct StreamOrder {
 // lowest-ranked corner, and hub rows stay short.
 __device__ __forceinline__ bool rank_above(uint32_t a, uint32_t da, uint32_t b, uint32_t db) {
   return db > da || (db == da && b > a);
+}
+
+// The shared-position mask of owner's H2H entry for neighbour key (present
+// by construction): a binary search of the owner's id-sorted row. The
+// oriented rows keep no mask of their own.
+__device__ __forceinline__ uint64_t row_mask(const uint64_t* off, const uint32_t* len, const uint32_t* nbr,
+                                             const uint64_t* mask, uint32_t owner, uint32_t key) {
+  const uint64_t s = off[owner];
+  uint32_t lo = 0, hi = len[owner];
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(nbr + s + mid) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return __ldg(mask + s + lo);
 }
 #endif
 

@@ -145,7 +145,7 @@ struct ClosedArgs {
   const uint32_t* plen;
   const uint32_t* pnbr;
   const uint16_t* pos;    // (neighbour size << 8) | overlap
-  const uint32_t* prel;   // each entry's index in its owner's H2H row
+  const uint32_t* rnbr;   // H2H neighbour ids (a centre's masks are looked up in its H2H row)
   const uint64_t* hoff;   // H2V
   const uint32_t* hmem;
   const uint8_t* esize;
@@ -165,10 +165,11 @@ struct ClosedArgs {
   const uint4* wtab;        // per group: {start in the row, size-1 neighbours, size-2 neighbours, 0}
   const uint8_t* wopos;     // per oriented entry (a, b), id-sorted: position in b of the one member
                             // a and b share, 0xff if they share several or it is past 63
-  // H2H offsets and shared-position masks (the row owner's members < 64),
-  // read through prel
+  // H2H offsets, masks (the row owner's members < 64), lengths, overlaps
   const uint64_t* roff;
   const uint64_t* rmask;
+  const uint32_t* rlen;
+  const uint8_t* rovl;
 };
 
 constexpr uint32_t kGroupPositions = 64;
@@ -237,27 +238,57 @@ struct CentreTable {
   bool skip;
 };
 
+__device__ __forceinline__ void table_insert(uint32_t* keys, uint64_t* sval, uint32_t shift, uint32_t bmask,
+                                             uint32_t key, uint64_t value) {
+  uint32_t bk = hash_slot(key, shift), h = 0;
+  for (bool done = false; !done; bk = (bk + 1) & bmask)
+    for (uint32_t t = 0; t < 4; ++t)
+      if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
+        h = 4 * bk + t;
+        done = true;
+        break;
+      }
+  sval[h] = value;
+}
+
 // Fills the table with N+(a), threads t = first, first + stride, ...; the
 // masks of the entries sharing two or more members with a are ORed into
-// *heavy_or (when given).
-__device__ __forceinline__ void fill_table(const ClosedArgs& A, const uint64_t* amask, uint64_t ao, uint32_t ad,
-                                           uint32_t* keys,
-                                           uint64_t* sval, uint32_t shift, uint32_t bmask, bool flags, bool exact,
-                                           unsigned first, unsigned stride, unsigned long long* heavy_or) {
-  for (uint32_t i = first; i < ad; i += stride) {
-    const uint32_t key = A.pnbr[ao + i];
-    uint32_t bk = hash_slot(key, shift), h = 0;
-    for (bool done = false; !done; bk = (bk + 1) & bmask)
-      for (uint32_t t = 0; t < 4; ++t)
-        if (atomicCAS(&keys[4 * bk + t], kEmpty, key) == kEmpty) {
-          h = 4 * bk + t;
-          done = true;
-          break;
-        }
-    const uint64_t m = exact ? amask[A.prel[ao + i]] : 0;
-    sval[h] = flags ? (uint64_t)i : exact ? m : (uint64_t)(A.pos[ao + i] & 0xffu);
-    if (heavy_or && exact && (A.pos[ao + i] & 0xffu) >= 2u) atomicOr(heavy_or, (unsigned long long)m);
+// *heavy_or (when given). Counts read N+(a) from a's H2H row, the entries
+// ranked above a (the oriented rows' own rule), so each entry's overlap and
+// mask come with it. Diagnostics (flags) read the oriented row and store each
+// entry's index.
+__device__ __forceinline__ void fill_table(const ClosedArgs& A, uint32_t a, uint64_t ao, uint32_t ad,
+                                           uint32_t* keys, uint64_t* sval, uint32_t shift, uint32_t bmask,
+                                           bool flags, bool exact, unsigned first, unsigned stride,
+                                           unsigned long long* heavy_or) {
+  if (flags) {
+    for (uint32_t i = first; i < ad; i += stride) table_insert(keys, sval, shift, bmask, A.pnbr[ao + i], i);
+    return;
   }
+  const uint64_t ro = A.roff[a];
+  const uint32_t rd = A.rlen[a];
+  for (uint32_t i = first; i < rd; i += stride) {
+    const uint32_t key = __ldg(A.rnbr + ro + i);
+    if (!rank_above(a, rd, key, __ldg(A.rlen + key))) continue;
+    const uint32_t ov = __ldg(A.rovl + ro + i);
+    const uint64_t m = exact ? __ldg(A.rmask + ro + i) : 0;
+    table_insert(keys, sval, shift, bmask, key, exact ? m : (uint64_t)ov);
+    if (heavy_or && exact && ov >= 2u) atomicOr(heavy_or, (unsigned long long)m);
+  }
+}
+
+// The value the centre's shared table holds for key, a member of N+(a) (so
+// present; the probe is bounded by the table size all the same, and a key
+// not found has its mask read from the H2H row).
+__device__ __forceinline__ uint64_t table_value(const ClosedArgs& A, const CentreTable& T, uint32_t a, uint32_t key) {
+  uint32_t bk = hash_slot(key, T.shift);
+  for (uint32_t n = 0; n <= T.bmask; ++n) {
+    const uint4 q = reinterpret_cast<const uint4*>(T.keys)[bk];
+    const int t = q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : q.w == key ? 3 : -1;
+    if (t >= 0) return T.sval[4 * bk + (uint32_t)t];
+    bk = (bk + 1) & T.bmask;
+  }
+  return row_mask(A.roff, A.rlen, A.rnbr, A.rmask, a, key);
 }
 
 // Whole warp, converged: the lanes with push set append their record to the
@@ -297,8 +328,11 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   const uint32_t b = A.pnbr[ao + bi];
   const uint32_t osb = A.pos[ao + bi];
   const uint32_t cab = osb & 0xffu, sb = osb >> 8;
-  const uint64_t* amask = A.rmask + A.roff[a];
-  const uint64_t mab = amask[A.prel[ao + bi]];
+  // the mask of (a, b): from the centre's table (it holds masks when a has at
+  // most 64 members), else from a's H2H row
+  const uint64_t mab = !exact_masks              ? 0
+                       : (T.in_smem && !flags) ? table_value(A, T, a, b)
+                                               : row_mask(A.roff, A.rlen, A.rnbr, A.rmask, a, b);
   const uint64_t bo = A.poff[b];
   const uint32_t bd = A.plen[b];
   // N+(b) is walked in its grouped copy when there is one (any order of a
@@ -333,18 +367,31 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
   }
   const uint32_t bdw = bd - glen;  // entries walked
   // kUnroll probes per lane per round: their id and overlap/size loads are
-  // issued together so several global loads are in flight per lane.
+  // issued together, and the next round's before this round's probes, so
+  // that the walk's global loads overlap the probing (software pipelining).
+  uint32_t cv[kUnroll], ov[kUnroll];
+#pragma unroll
+  for (unsigned u = 0; u < kUnroll; ++u) {
+    const uint32_t j = u * kWarp + lane;
+    cv[u] = kEmpty;
+    ov[u] = 0;
+    if (j < bdw) {
+      const uint32_t jj = j < gs ? j : j + glen;
+      cv[u] = __ldg(wnbr + bo + jj);
+      ov[u] = __ldg(wos + bo + jj);
+    }
+  }
   for (uint32_t j0 = 0; j0 < bdw; j0 += kWarp * kUnroll) {
-    uint32_t cv[kUnroll], ov[kUnroll];
+    uint32_t cn[kUnroll], on[kUnroll];
 #pragma unroll
     for (unsigned u = 0; u < kUnroll; ++u) {
-      const uint32_t j = j0 + u * kWarp + lane;
-      cv[u] = kEmpty;
-      ov[u] = 0;
+      const uint32_t j = j0 + kWarp * kUnroll + u * kWarp + lane;
+      cn[u] = kEmpty;
+      on[u] = 0;
       if (j < bdw) {
         const uint32_t jj = j < gs ? j : j + glen;
-        cv[u] = __ldg(wnbr + bo + jj);
-        ov[u] = __ldg(wos + bo + jj);
+        cn[u] = __ldg(wnbr + bo + jj);
+        on[u] = __ldg(wos + bo + jj);
       }
     }
 #pragma unroll
@@ -373,7 +420,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
             A.edge_flags[ao + bi] = 1;
             A.edge_flags[bo + j] = 1;
             cac = A.pos[ao + v] & 0xffu;
-            mac = amask[A.prel[ao + v]];
+            mac = row_mask(A.roff, A.rlen, A.rnbr, A.rmask, a, c);
           } else if (exact_masks) {
             mac = v;
             cac = (uint32_t)__popcll(v);
@@ -391,7 +438,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
         }
         if (lo < ad && row[lo] == c) {
           cac = A.pos[ao + lo] & 0xffu;
-          mac = amask[A.prel[ao + lo]];
+          mac = row_mask(A.roff, A.rlen, A.rnbr, A.rmask, a, c);
           if (flags) {
             const uint32_t j = j0 + u * kWarp + lane;
             A.edge_flags[ao + lo] = 1;
@@ -425,6 +472,11 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
       rec = pack_triangle(sb, sc, cab, cbc, cac, g);
       } while (false);
       if (!kTriads) queue_push(push, rec, q, qn, sa, wc);  // warp-converged
+    }
+#pragma unroll
+    for (unsigned u = 0; u < kUnroll; ++u) {
+      cv[u] = cn[u];
+      ov[u] = on[u];
     }
   }
   if (kTriads) {
@@ -509,7 +561,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
       T.bmask = buckets - 1;
       for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) keys[i] = kEmpty;
       __syncthreads();
-      fill_table(A, A.rmask + A.roff[a], ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x,
+      fill_table(A, a, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, threadIdx.x,
                  blockDim.x, &s_heavy);
     }
     __syncthreads();
@@ -575,7 +627,7 @@ __global__ void __launch_bounds__(kClosedBlock, 4) k_closed_warp(ClosedArgs A) {
     for (uint32_t i = lane; i < slots; i += kWarp) keys[i] = kEmpty;
     if (lane == 0) heavy_all[w] = 0;
     __syncwarp();
-    fill_table(A, A.rmask + A.roff[a], ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp,
+    fill_table(A, a, ao, ad, keys, sval, T.shift, T.bmask, flags, sa <= 64, lane, kWarp,
                &heavy_all[w]);
     __syncwarp();
     const uint32_t cat_a = size_cat(sa);
@@ -706,8 +758,11 @@ static int prepare_static_attrs() {
 // The grouped rows and the rank the closed phase's walk uses (left null,
 // the walk takes the id-sorted rows and skips nothing).
 static void with_masks(const hm_graph* g, ClosedArgs& A) {
+  A.rnbr = g->h2h_nbr.p;
   A.roff = g->h2h_off.p;
   A.rmask = g->h2h_mask.p;
+  A.rlen = g->h2h_len.p;
+  A.rovl = g->h2h_ovl.p;
 }
 
 static void with_groups(const hm_graph* g, ClosedArgs& A) {
@@ -806,7 +861,7 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   const uint32_t E = g->n_slots;
   unsigned long long* dev = g->counters.p;
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p,
+  ClosedArgs args{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->h2h_nbr.p,
                   g->h2v_off.p,  g->h2v_mem.p,  g->esize.p,    g->work.p,    0,
                   shard,         n_shards,      nullptr,       dev,          edge_flags,
                   nullptr,       nullptr};
@@ -835,7 +890,7 @@ int launch_static(hm_graph* g, uint32_t shard, uint32_t n_shards, uint8_t* edge_
   const uint64_t key[CountCapture::kKey] = {
       (uint64_t)g->h2h_off.p,  (uint64_t)g->h2h_len.p,  (uint64_t)g->h2h_nbr.p,   (uint64_t)g->h2h_ovl.p,
       (uint64_t)g->esize.p,    (uint64_t)g->plus_off.p, (uint64_t)g->plus_len.p,  (uint64_t)g->plus_nbr.p,
-      (uint64_t)g->plus_os.p,  (uint64_t)g->plus_rel.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
+      (uint64_t)g->plus_os.p,  (uint64_t)g->h2h_nbr.p, (uint64_t)g->h2v_off.p,  (uint64_t)g->h2v_mem.p,
       (uint64_t)g->work.p,     (uint64_t)dev,            E,                       g->n_work,
       g->n_work_big,           g->n_work_mid,            shard,                   n_shards,
       (uint64_t)args.wnbr,     (uint64_t)args.wos,       (uint64_t)args.wbase,    (uint64_t)args.wtab,
@@ -1005,7 +1060,7 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   HM_CUDA(cudaStreamSynchronize(st));
   const uint32_t n_work = hw[0], n_big = hw[1];
   const uint32_t bounds[4] = {0, n_big, hw[2], n_work};
-  ClosedArgs pargs{P.off.p, P.len.p, P.nbr.p, P.os.p, P.rel.p, g->h2v_off.p, g->h2v_mem.p,
+  ClosedArgs pargs{P.off.p, P.len.p, P.nbr.p, P.os.p, g->h2h_nbr.p, g->h2v_off.p, g->h2v_mem.p,
                    g->esize.p, work.p, 0, 0, 1, nullptr, cnt.p, nullptr, rows.gos, rows.rog};
   with_masks(g, pargs);
   HM_TRY(launch_closed(ctx, pargs, bounds, reinterpret_cast<unsigned int*>(tail)));
@@ -1067,7 +1122,7 @@ int count_vertex_triads(hm_graph* g, uint64_t out3[3]) {
     HM_LAUNCH_CHECK();
   }
   const uint32_t bounds[4] = {0, g->n_work_big, g->n_work_mid, g->n_work};
-  ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2v_off.p,
+  ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->h2h_nbr.p, g->h2v_off.p,
                    g->h2v_mem.p,    g->esize.p,    g->work.p,      0,             0,               1,
                    nullptr,         cnt.p,         nullptr,        nullptr,       nullptr};
   with_masks(g, targs);
@@ -1191,7 +1246,7 @@ int autotune_closed(hm_graph* g, uint32_t stride, hm_tune_report& R) {
       HM_CUDA(cudaMemcpyAsync(hw, wc, sizeof(hw), cudaMemcpyDeviceToHost, st));
       HM_CUDA(cudaStreamSynchronize(st));
       const uint32_t bounds[4] = {0, hw[1], hw[2], hw[0]};
-      ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2v_off.p,
+      ClosedArgs targs{g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->h2h_nbr.p, g->h2v_off.p,
                        g->h2v_mem.p,    g->esize.p,    work.p,         0,             0,               1,
                        nullptr,         cnt.p,         nullptr,        nullptr,       nullptr};
       with_groups(g, targs);

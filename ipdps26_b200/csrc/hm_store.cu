@@ -264,7 +264,7 @@ __global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uin
 
 __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint8_t* ovl,
                              const uint8_t* esize, const uint32_t* rows, uint32_t n, const uint64_t* poff,
-                             uint32_t* pnbr, uint16_t* pos, uint32_t* prel) {
+                             uint32_t* pnbr, uint16_t* pos) {
   for (uint64_t r = global_warp(); r < n; r += n_warps()) {
     const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint64_t s = off[a];
@@ -283,7 +283,6 @@ __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uin
         const uint64_t d = w + __popc(m & lanemask_lt());
         pnbr[d] = b;
         pos[d] = (uint16_t)(((uint32_t)esize[b] << 8) | ovl[s + i]);
-        prel[d] = i;
       }
       w += __popc(m);
     }
@@ -310,8 +309,9 @@ __global__ void k_group_sizes(const uint8_t* esize, uint32_t n, uint32_t* tsize)
 constexpr unsigned kGroupWarps = kBlock / kWarp;
 __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, const uint32_t* plen,
                                                        const uint32_t* pnbr, const uint16_t* pos,
-                                                       const uint32_t* prel, const uint64_t* roff,
-                                                       const uint64_t* rmask, const uint8_t* esize, uint32_t n,
+                                                       const uint64_t* roff, const uint32_t* rlen,
+                                                       const uint32_t* rnbr, const uint64_t* rmask,
+                                                       const uint8_t* esize, uint32_t n,
                                                        const uint64_t* gbase, uint4* gtab, uint32_t* gnbr,
                                                        uint16_t* gos) {
   __shared__ uint32_t cnt[kGroupWarps][kGroupPositions + 1];
@@ -324,10 +324,9 @@ __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, con
     __syncwarp();
     const uint64_t s = poff[b];
     const uint32_t l = plen[b];
-    const uint64_t* bmask = rmask + roff[b];
     for (uint32_t i = lane; i < l; i += kWarp) {
       const uint16_t o = pos[s + i];
-      const uint32_t grp = group_of(o, bmask[prel[s + i]]);  // < G: a position bit p < min(size, 64)
+      const uint32_t grp = group_of(o, row_mask(roff, rlen, rnbr, rmask, (uint32_t)b, pnbr[s + i]));  // < G: a position bit p < min(size, 64)
       atomicAdd(&cnt[w][grp], 1u);
       const uint32_t sc = o >> 8;
       if (sc == 1) atomicAdd(&one[w][grp], 1u);
@@ -348,7 +347,8 @@ __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, con
     __syncwarp();
     for (uint32_t i = lane; i < l; i += kWarp) {
       const uint16_t o = pos[s + i];
-      const uint32_t d = atomicAdd(&cnt[w][group_of(o, bmask[prel[s + i]])], 1u);
+      const uint32_t d =
+          atomicAdd(&cnt[w][group_of(o, row_mask(roff, rlen, rnbr, rmask, (uint32_t)b, pnbr[s + i]))], 1u);
       gnbr[s + d] = pnbr[s + i];
       gos[s + d] = o;
     }
@@ -361,15 +361,15 @@ __global__ void __launch_bounds__(kBlock) k_group_rows(const uint64_t* poff, con
 // (a binary search of b's sorted members), 0xff for every other entry and
 // for a position of 64 or more in b.
 __global__ void k_shared_positions(const uint64_t* poff, const uint32_t* plen, const uint32_t* pnbr,
-                                   const uint16_t* pos, const uint32_t* prel, const uint64_t* roff,
-                                   const uint64_t* rmask, const uint64_t* hoff, const uint32_t* hmem,
+                                   const uint16_t* pos, const uint64_t* roff, const uint32_t* rlen,
+                                   const uint32_t* rnbr, const uint64_t* rmask, const uint64_t* hoff,
+                                   const uint32_t* hmem,
                                    const uint8_t* esize, uint32_t n, uint8_t* opos) {
   for (uint64_t a = global_warp(); a < n; a += n_warps()) {
     const uint64_t s = poff[a];
     const uint32_t* am = hmem + hoff[a];
-    const uint64_t* amask = rmask + roff[a];
     for (uint32_t i = lane_id(); i < plen[a]; i += kWarp) {
-      const uint64_t m = amask[prel[s + i]];
+      const uint64_t m = row_mask(roff, rlen, rnbr, rmask, (uint32_t)a, pnbr[s + i]);
       uint8_t p = 0xff;
       if ((pos[s + i] & 0xffu) == 1u && m) {
         const uint32_t u = am[__ffsll((long long)m) - 1];
@@ -412,12 +412,12 @@ int build_plus_groups(hm_graph* g) {
   HM_TRY(g->grp_os.alloc(ctx, g->plus_nnz));
   if (E) {
     k_group_rows<<<grid_for((uint64_t)E * kWarp, kBlock), kBlock, 0, st>>>(
-        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2h_off.p, g->h2h_mask.p,
-        g->esize.p, E, g->grp_base.p, g->grp_tab.p, g->grp_nbr.p, g->grp_os.p);
+        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+        g->h2h_mask.p, g->esize.p, E, g->grp_base.p, g->grp_tab.p, g->grp_nbr.p, g->grp_os.p);
     HM_LAUNCH_CHECK();
     k_shared_positions<<<grid_for((uint64_t)E * kWarp, kBlock), kBlock, 0, st>>>(
-        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->plus_rel.p, g->h2h_off.p, g->h2h_mask.p,
-        g->h2v_off.p, g->h2v_mem.p, g->esize.p, E, g->grp_opos.p);
+        g->plus_off.p, g->plus_len.p, g->plus_nbr.p, g->plus_os.p, g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
+        g->h2h_mask.p, g->h2v_off.p, g->h2v_mem.p, g->esize.p, E, g->grp_opos.p);
     HM_LAUNCH_CHECK();
   }
   g->grp_valid = true;
@@ -428,7 +428,6 @@ int build_plus_groups(hm_graph* g) {
 void release_plus(hm_graph* g) {
   g->plus_nbr.release();
   g->plus_os.release();
-  g->plus_rel.release();
   g->plus_valid = false;
   release_plus_groups(g);
 }
@@ -747,13 +746,12 @@ int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P
   HM_CUDA(cudaStreamSynchronize(st));
   HM_TRY(P->nbr.alloc(ctx, total));
   HM_TRY(P->os.alloc(ctx, total));
-  HM_TRY(P->rel.alloc(ctx, total));
   if (n) {
     k_plus_scatter<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_rows, n, pos.p, cnt.p, P->off.p, P->len.p);
     HM_LAUNCH_CHECK();
     k_plus_write<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
                                                                       g->h2h_ovl.p, g->esize.p, d_rows, n, P->off.p,
-                                                                      P->nbr.p, P->os.p, P->rel.p);
+                                                                      P->nbr.p, P->os.p);
     HM_LAUNCH_CHECK();
   }
   P->nnz = total;
@@ -790,12 +788,10 @@ static int build_plus_once(hm_graph* g) {
   HM_CUDA(cudaStreamSynchronize(st));
   HM_TRY(g->plus_nbr.alloc(ctx, total));
   HM_TRY(g->plus_os.alloc(ctx, total));
-  HM_TRY(g->plus_rel.alloc(ctx, total));
   if (E) {
     k_plus_write<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
                                                                       g->h2h_ovl.p, g->esize.p, nullptr, E,
-                                                                      g->plus_off.p, g->plus_nbr.p, g->plus_os.p,
-                                                                      g->plus_rel.p);
+                                                                      g->plus_off.p, g->plus_nbr.p, g->plus_os.p);
     HM_LAUNCH_CHECK();
   }
   g->plus_len = static_cast<DArr<uint32_t>&&>(cnt);

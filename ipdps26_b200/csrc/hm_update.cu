@@ -529,19 +529,22 @@ static int compact_h2h(hm_graph* g, uint64_t extra) {
   release_plus(g);
   HM_TRY(compact_h2h_in_place(g));
   const uint64_t live = g->h2h_tail;
-  // Keep about half the live size free after a compaction, so that a batch
-  // needs few of them, but leave the device room for what the store
-  // needs besides the arena: the oriented copy of a count (10 bytes for
-  // each of about live / 2 entries) and a batch's scratch. Under that
-  // pressure the arena only grows to the least that serves this request
-  // (later batches compact more often).
-  if (live + std::max<uint64_t>(extra, live / 2) <= g->h2h_cap) return HM_OK;
+  // Keep about half the live size free after a compaction (at most a tenth
+  // of the budget), so that a batch needs few of them, but leave the device
+  // room for what the store needs besides the arena: the oriented copy of a
+  // count (6 bytes for each of about live / 2 entries), a batch's scratch
+  // and the stream-ordered pool's slack (a sixteenth of the budget). Under
+  // that pressure the arena only grows to the least that serves this
+  // request (later batches compact more often).
+  uint64_t slack = live / 2;
+  if (ctx->budget) slack = std::min<uint64_t>(slack, ctx->budget / 10 / 13);
+  if (live + std::max<uint64_t>(extra, slack) <= g->h2h_cap) return HM_OK;
   const uint64_t lean = live + extra + (live + extra) / 32 + 1024;
-  uint64_t want = std::max<uint64_t>(live + live / 2, live + extra + (live + extra) / 8) + 1024;
+  uint64_t want = std::max<uint64_t>(live + slack, live + extra + (live + extra) / 8) + 1024;
   if (ctx->budget) {
     const size_t arena = g->h2h_nbr.bytes() + g->h2h_ovl.bytes() + g->h2h_mask.bytes();
     const size_t other = ctx->used.load() - std::min<size_t>(ctx->used.load(), arena);
-    const size_t reserve = (size_t)(live / 2) * 10 + (size_t(8) << 30);
+    const size_t reserve = (size_t)(live / 2) * 6 + ctx->budget / 16;
     const size_t room = ctx->budget > other + reserve ? ctx->budget - other - reserve : 0;
     want = std::min<uint64_t>(want, room / 13);
   }
@@ -706,6 +709,7 @@ int apply_batch_hooks(hm_graph* g, const uint32_t* h_dels, uint32_t n_del, const
   trace.mark("validate");
   if (hooks.before) HM_TRY(hooks.before(dels.p, n_del));
   trace.mark("count_deleted");
+  release_plus(g);  // the old graph's oriented rows: not used again, and the patching needs the room
 
   // ---- deletions: H2H removal patches from the rows about to vanish ----------
   DArr<uint64_t> rem_off;
