@@ -235,6 +235,10 @@ struct hm_graph {
   hm::DArr<uint32_t> plus_nbr;
   hm::DArr<uint16_t> plus_os;  // (neighbour size << 8) | overlap
   uint64_t plus_nnz = 0;
+  // the masks of the oriented rows longer than kLongRow, which the count
+  // kernels search instead of tabling: per slot its start in long_mask
+  hm::DArr<uint64_t> long_off;
+  hm::DArr<uint64_t> long_mask;
   // The oriented rows once more, grouped for the static count's walk: in
   // each row, first the neighbours that share several members with the row
   // owner (or one at a position past 63 of its member list), then one group
@@ -307,8 +311,13 @@ struct PlusRows {
   DArr<uint32_t> len;
   DArr<uint32_t> nbr;
   DArr<uint16_t> os;
+  DArr<uint64_t> loff;   // masks of the rows longer than kLongRow, as hm_graph::long_off
+  DArr<uint64_t> lmask;
   uint64_t nnz = 0;
 };
+// Oriented rows longer than this are searched, not tabled, by the count
+// kernels (the largest shared-memory table holds 4096 entries).
+constexpr uint32_t kLongRow = 4096;
 int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P);
 template <class T>
 int exclusive_scan(hm_ctx* ctx, const T* in, uint64_t* out, uint64_t n);

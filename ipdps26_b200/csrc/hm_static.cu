@@ -170,6 +170,9 @@ struct ClosedArgs {
   const uint64_t* rmask;
   const uint32_t* rlen;
   const uint8_t* rovl;
+  // masks of the oriented rows longer than kLongRow (hm_graph::long_off)
+  const uint64_t* loff;
+  const uint64_t* lmask;
 };
 
 constexpr uint32_t kGroupPositions = 64;
@@ -429,6 +432,9 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
           }
         }
       } else {
+        // rows too long for the table (longer than kLongRow: every kernel
+        // tables all rows shorter than that it can be given): a search of
+        // N+(a), whose masks are kept beside it
         uint32_t lo = 0, hi = ad;
         const uint32_t* row = A.pnbr + ao;
         while (lo < hi) {
@@ -438,7 +444,7 @@ __device__ __forceinline__ void closed_pairs_of_b(const ClosedArgs& A, uint32_t 
         }
         if (lo < ad && row[lo] == c) {
           cac = A.pos[ao + lo] & 0xffu;
-          mac = row_mask(A.roff, A.rlen, A.rnbr, A.rmask, a, c);
+          mac = exact_masks ? A.lmask[A.loff[a] + lo] : 0;
           if (flags) {
             const uint32_t j = j0 + u * kWarp + lane;
             A.edge_flags[ao + lo] = 1;
@@ -518,6 +524,9 @@ template <unsigned kHashSlotsMax, unsigned kMinBlocks, bool kTriads = false>
 __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
   static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
   constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
+  // rows not tabled must have their masks kept (longer than kLongRow), or
+  // never reach this shape (the schedule sends it rows up to kSmallRow)
+  static_assert(kHashRowMax == kLongRow || kHashRowMax >= kSmallRow, "untabled rows without masks");
   extern __shared__ uint64_t smem64[];
   uint64_t* sval = smem64;                                             // kHashSlotsMax
   uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kHashSlotsMax);  // kHashSlotsMax
@@ -763,6 +772,8 @@ static void with_masks(const hm_graph* g, ClosedArgs& A) {
   A.rmask = g->h2h_mask.p;
   A.rlen = g->h2h_len.p;
   A.rovl = g->h2h_ovl.p;
+  A.loff = g->long_off.p;
+  A.lmask = g->long_mask.p;
 }
 
 static void with_groups(const hm_graph* g, ClosedArgs& A) {
@@ -1063,6 +1074,8 @@ int count_static_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, const Tou
   ClosedArgs pargs{P.off.p, P.len.p, P.nbr.p, P.os.p, g->h2h_nbr.p, g->h2v_off.p, g->h2v_mem.p,
                    g->esize.p, work.p, 0, 0, 1, nullptr, cnt.p, nullptr, rows.gos, rows.rog};
   with_masks(g, pargs);
+  pargs.loff = P.loff.p;
+  pargs.lmask = P.lmask.p;
   HM_TRY(launch_closed(ctx, pargs, bounds, reinterpret_cast<unsigned int*>(tail)));
   std::vector<unsigned long long> h((size_t)R * kRowStride);
   HM_CUDA(cudaMemcpyAsync(h.data(), cnt.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));

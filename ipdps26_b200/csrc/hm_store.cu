@@ -263,13 +263,16 @@ __global__ void k_plus_count(const uint64_t* off, const uint32_t* len, const uin
 }
 
 __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uint32_t* nbr, const uint8_t* ovl,
-                             const uint8_t* esize, const uint32_t* rows, uint32_t n, const uint64_t* poff,
-                             uint32_t* pnbr, uint16_t* pos) {
+                             const uint64_t* mask, const uint8_t* esize, const uint32_t* rows, uint32_t n,
+                             const uint64_t* poff, const uint32_t* plen, const uint64_t* loff, uint32_t* pnbr,
+                             uint16_t* pos, uint64_t* lmask) {
   for (uint64_t r = global_warp(); r < n; r += n_warps()) {
     const uint32_t a = rows ? rows[r] : (uint32_t)r;
     const uint64_t s = off[a];
     const uint32_t l = len[a];
-    uint64_t w = poff[a];
+    const uint64_t w0 = poff[a];
+    const bool long_row = plen[a] > kLongRow;
+    uint64_t w = w0;
     for (uint32_t i0 = 0; i0 < l; i0 += kWarp) {
       const uint32_t i = i0 + lane_id();
       bool up = false;
@@ -283,6 +286,7 @@ __global__ void k_plus_write(const uint64_t* off, const uint32_t* len, const uin
         const uint64_t d = w + __popc(m & lanemask_lt());
         pnbr[d] = b;
         pos[d] = (uint16_t)(((uint32_t)esize[b] << 8) | ovl[s + i]);
+        if (long_row) lmask[loff[a] + (d - w0)] = mask[s + i];
       }
       w += __popc(m);
     }
@@ -426,6 +430,8 @@ int build_plus_groups(hm_graph* g) {
 
 // Frees the oriented copy (and the grouped one built from it).
 void release_plus(hm_graph* g) {
+  g->long_off.release();
+  g->long_mask.release();
   g->plus_nbr.release();
   g->plus_os.release();
   g->plus_valid = false;
@@ -715,6 +721,46 @@ int build_h2h_rows(hm_graph* g) {
   return HM_OK;
 }
 
+// The long rows' lengths (0 for the others), per listed row (rows null: slots).
+__global__ void k_long_len(const uint32_t* cnt, uint32_t n, uint32_t* llen) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    llen[i] = cnt[i] > kLongRow ? cnt[i] : 0u;
+}
+
+__global__ void k_long_scatter(const uint32_t* rows, uint32_t n, const uint64_t* lpos, uint64_t* loff) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    loff[rows[i]] = lpos[i];
+}
+
+// The long rows' mask offsets (per slot) and their mask array; returns its size.
+static int long_rows(hm_ctx* ctx, const uint32_t* rows, uint32_t n, const uint32_t* cnt, uint32_t n_slots,
+                     DArr<uint64_t>* loff, DArr<uint64_t>* lmask) {
+  cudaStream_t st = ctx->stream;
+  DArr<uint32_t> llen;
+  DArr<uint64_t> lpos;
+  HM_TRY(llen.alloc(ctx, n));
+  HM_TRY(lpos.alloc(ctx, (size_t)n + 1));
+  if (n) {
+    k_long_len<<<grid_for(n, kBlock), kBlock, 0, st>>>(cnt, n, llen.p);
+    HM_LAUNCH_CHECK();
+  }
+  HM_TRY(exclusive_scan(ctx, llen.p, lpos.p, n));
+  uint64_t total = 0;
+  HM_CUDA(cudaMemcpyAsync(&total, lpos.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  HM_CUDA(cudaStreamSynchronize(st));
+  HM_TRY(lmask->alloc(ctx, total));
+  if (!rows) {
+    *loff = static_cast<DArr<uint64_t>&&>(lpos);
+    return HM_OK;
+  }
+  HM_TRY(loff->alloc(ctx, (size_t)n_slots + 1));
+  if (n) {
+    k_long_scatter<<<grid_for(n, kBlock), kBlock, 0, st>>>(rows, n, lpos.p, loff->p);
+    HM_LAUNCH_CHECK();
+  }
+  return HM_OK;
+}
+
 __global__ void k_plus_scatter(const uint32_t* rows, uint32_t n, const uint64_t* pos, const uint32_t* cnt,
                                uint64_t* poff, uint32_t* plen) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -746,12 +792,13 @@ int build_plus_rows(hm_graph* g, const uint32_t* d_rows, uint32_t n, PlusRows* P
   HM_CUDA(cudaStreamSynchronize(st));
   HM_TRY(P->nbr.alloc(ctx, total));
   HM_TRY(P->os.alloc(ctx, total));
+  HM_TRY(long_rows(ctx, d_rows, n, cnt.p, g->n_slots, &P->loff, &P->lmask));
   if (n) {
     k_plus_scatter<<<grid_for(n, kBlock), kBlock, 0, st>>>(d_rows, n, pos.p, cnt.p, P->off.p, P->len.p);
     HM_LAUNCH_CHECK();
-    k_plus_write<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
-                                                                      g->h2h_ovl.p, g->esize.p, d_rows, n, P->off.p,
-                                                                      P->nbr.p, P->os.p);
+    k_plus_write<<<grid_for((uint64_t)n * 32, kBlock), kBlock, 0, st>>>(
+        g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p, g->esize.p, d_rows, n, P->off.p,
+        P->len.p, P->loff.p, P->nbr.p, P->os.p, P->lmask.p);
     HM_LAUNCH_CHECK();
   }
   P->nnz = total;
@@ -788,10 +835,11 @@ static int build_plus_once(hm_graph* g) {
   HM_CUDA(cudaStreamSynchronize(st));
   HM_TRY(g->plus_nbr.alloc(ctx, total));
   HM_TRY(g->plus_os.alloc(ctx, total));
+  HM_TRY(long_rows(ctx, nullptr, E, cnt.p, E, &g->long_off, &g->long_mask));
   if (E) {
-    k_plus_write<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p,
-                                                                      g->h2h_ovl.p, g->esize.p, nullptr, E,
-                                                                      g->plus_off.p, g->plus_nbr.p, g->plus_os.p);
+    k_plus_write<<<grid_for((uint64_t)E * 32, kBlock), kBlock, 0, st>>>(
+        g->h2h_off.p, g->h2h_len.p, g->h2h_nbr.p, g->h2h_ovl.p, g->h2h_mask.p, g->esize.p, nullptr, E,
+        g->plus_off.p, cnt.p, g->long_off.p, g->plus_nbr.p, g->plus_os.p, g->long_mask.p);
     HM_LAUNCH_CHECK();
   }
   g->plus_len = static_cast<DArr<uint32_t>&&>(cnt);

@@ -249,3 +249,22 @@ def test_grouped_walk_equals_plain_walk_and_oracle(ctx, seed):
                 for on in (True, False):
                     g.set_static_groups(on)
                     assert g.count_static30().tolist() == want.tolist(), (sched, on)
+
+
+def test_oriented_rows_longer_than_the_table(ctx):
+    """A centre with more than 4,096 neighbours ranked above it is counted
+    without its shared-memory table (a filter in that memory, then a search of
+    its H2H row): hyperedge 0 = {0..9} and 4,200 hyperedges {z, i mod 10,
+    1000 + i} of equal degree above it. Checked against the touched-triple
+    count of every hyperedge (other kernels, a count of the same triples)."""
+    from ipdps26_b200 import engine
+
+    z = 999
+    rows = [list(range(10))] + [sorted({z, i % 10, 1000 + i}) for i in range(4200)]
+    off, mem = csr(rows)
+    with engine.Graph(ctx, off, mem, 1000 + 4200) as g:
+        g.set_schedule(128, 2048)
+        full = g.count_static30()
+        every = g.count_touching30(np.arange(len(rows), dtype=np.uint32))
+        assert full.tolist() == every.tolist()
+        assert int(full.sum()) > 0
