@@ -279,7 +279,7 @@ int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, uint32_t n, 
  * decided by a strict comparison of their times, as THyMe compares them
  * (main_thymeP.cpp:313-323), a tie counting as "c before b" with b the
  * hyperedge of the pair whose node-set comes first in the input (THyMe's own
- * numbering, which its input shuffle randomises). HM_ERR_LIMIT if an event has more than 2048
+ * numbering, which its input shuffle randomises). HM_ERR_LIMIT if an event has more than 4096
  * distinct neighbours inside its window. There is no temporal counter of
  * these 96 motifs in the reference's GPU code (its 3-layer strict-increasing
  * kernel, temporalDynamicHMotif/src/temporal_count.cu:91-217, bins 30 classes
@@ -290,7 +290,7 @@ int hm_count_temporal(hm_graph* g, int64_t delta, uint64_t out96[HM_N_TEMPORAL_M
  * d_out96 (device memory) and work queued on `stream` afterwards sees them;
  * the call returns without waiting (the first count of a graph builds its
  * time-ordered index first and waits for that). If an event has more than
- * 2048 distinct neighbours inside its window, all 96 counts read 2^64 - 1
+ * 4096 distinct neighbours inside its window, all 96 counts read 2^64 - 1
  * (the synchronous call returns HM_ERR_LIMIT). HM_ERR_STATE if `stream` or
  * the context stream is being captured into a CUDA graph. The reference's
  * counters are host programs with no stream (THyMe-main/code/
@@ -344,7 +344,7 @@ int hm_graph_traffic(hm_graph* g, hm_traffic_t* t);
  * 8192-slot table. Touched-triple count (the delta of every update batch):
  * the same three shapes per marked hyperedge m by the length of its row:
  * <= touch_warp_row one warp (<= 128), <= touch_mid_row 4096-slot blocks
- * (touch_warp_row <= touch_mid_row <= 2048), longer rows 512-thread blocks
+ * (touch_warp_row <= touch_mid_row <= 2048), longer rows 1024-thread blocks
  * with a 16384-slot table or a global table. Counts never depend on the
  * schedule; speed does. Default {128, 2048, 128, 2048}. The reference has
  * one launch shape, a thread per hyperedge
@@ -380,7 +380,8 @@ typedef struct hm_tune_report {
  * all candidates, and keeps the fastest of each; a default stays unless
  * another is at least 2 % faster. Static count: the closed phase on a
  * strided sample of the centres (sample_stride 0: at most 65536 centres,
- * 1: all), CUDA-event time. Touched-triple count: the count of every n-th
+ * 1: all), CUDA-event time; the candidates vary warp_row only (small_row
+ * 2048), as a sparse sample misjudges which rows share N+ in L2. Touched-triple count: the count of every n-th
  * live hyperedge (about 4096 of them, as a deletion batch marks them).
  * report may be NULL. */
 int hm_graph_autotune(hm_graph* g, uint32_t sample_stride, hm_tune_report* report);
