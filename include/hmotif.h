@@ -279,8 +279,8 @@ int hm_count_touching30_noalloc(hm_graph* g, const uint32_t* d_ids, uint32_t n, 
  * decided by a strict comparison of their times, as THyMe compares them
  * (main_thymeP.cpp:313-323), a tie counting as "c before b" with b the
  * hyperedge of the pair whose node-set comes first in the input (THyMe's own
- * numbering, which its input shuffle randomises). HM_ERR_LIMIT if an event has more than 4096
- * distinct neighbours inside its window. There is no temporal counter of
+ * numbering, which its input shuffle randomises). HM_ERR_LIMIT if an event
+ * has more than 4096 distinct neighbours inside its window. There is no temporal counter of
  * these 96 motifs in the reference's GPU code (its 3-layer strict-increasing
  * kernel, temporalDynamicHMotif/src/temporal_count.cu:91-217, bins 30 classes
  * of a different definition). */
@@ -381,8 +381,9 @@ typedef struct hm_tune_report {
  * another is at least 2 % faster. Static count: the closed phase on a
  * strided sample of the centres (sample_stride 0: at most 65536 centres,
  * 1: all), CUDA-event time; the candidates vary warp_row only (small_row
- * 2048), as a sparse sample misjudges which rows share N+ in L2. Touched-triple count: the count of every n-th
- * live hyperedge (about 4096 of them, as a deletion batch marks them).
+ * 2048), as a sparse sample misjudges which rows share N+ in L2.
+ * Touched-triple count: the count of every n-th live hyperedge (about 4096
+ * of them, as a deletion batch marks them).
  * report may be NULL. */
 int hm_graph_autotune(hm_graph* g, uint32_t sample_stride, hm_tune_report* report);
 
