@@ -46,9 +46,10 @@ constexpr unsigned kClosedWarps = kClosedBlock / kWarp;
 constexpr unsigned kUnroll = 4;               // probes in flight per lane
 constexpr unsigned kNumCounters = 36;        // 30 closed classes + 6 open-pair classes
 // Block launch shapes of the closed phase: rows up to the schedule's
-// small_row with a 4096-slot bucketized table (4 blocks per SM), longer rows
-// with an 8192-slot table (2 per SM). kSmallRow is the largest small_row the
-// 4096-slot table holds in shared memory (load <= 1/2).
+// small_row with a 4096-slot bucketized table (4 blocks of 256 threads per
+// SM), longer rows with a 16384-slot table (one 1024-thread block per SM).
+// kSmallRow is the largest small_row the 4096-slot table holds in shared
+// memory (load <= 1/2).
 constexpr unsigned kSmallRow = 2048;
 // Rows up to the schedule's warp_row go to the warp-per-centre kernel; its
 // 256-slot table per warp holds at most kWarpRow entries (load <= 1/2).
@@ -520,8 +521,9 @@ constexpr uint32_t kNoRow = 0xffffffffu;
 // One block per centre a (the lowest-ranked corner of its triangles): N+(a)
 // in a shared-memory table (load <= 1/4 up to kHashSlotsMax / 2 entries,
 // else searched in global memory), each warp takes one b in N+(a) at a time.
-template <unsigned kHashSlotsMax, unsigned kMinBlocks, bool kTriads = false>
-__global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs A) {
+template <unsigned kHashSlotsMax, unsigned kMinBlocks, bool kTriads = false, unsigned kThreads = kClosedBlock>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_closed(ClosedArgs A) {
+  constexpr unsigned kWarpsB = kThreads / kWarp;
   static_assert(kHashSlotsMax % 4 == 0, "whole buckets");
   constexpr unsigned kHashRowMax = kHashSlotsMax / 2;
   // rows not tabled must have their masks kept (longer than kLongRow), or
@@ -530,8 +532,8 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
   extern __shared__ uint64_t smem64[];
   uint64_t* sval = smem64;                                             // kHashSlotsMax
   uint32_t* keys = reinterpret_cast<uint32_t*>(sval + kHashSlotsMax);  // kHashSlotsMax
-  __shared__ unsigned long long wcnt[kClosedWarps][kNumCounters];
-  __shared__ uint64_t wqueue[kClosedWarps][2 * kWarp];  // per warp: triangles waiting to be classified
+  __shared__ unsigned long long wcnt[kWarpsB][kNumCounters];
+  __shared__ uint64_t wqueue[kWarpsB][2 * kWarp];  // per warp: triangles waiting to be classified
   __shared__ unsigned long long s_heavy;
   __shared__ uint32_t s_item;
   const unsigned w = threadIdx.x / kWarp, lane = lane_id();
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(kClosedBlock, kMinBlocks) k_closed(ClosedArgs 
     const bool exact_masks = sa <= 64;
     T.heavy_or = s_heavy;
     T.skip = T.in_smem && exact_masks && !flags && A.wnbr;
-    for (uint32_t bi = w; bi < ad; bi += kClosedWarps) {
+    for (uint32_t bi = w; bi < ad; bi += kWarpsB) {
       closed_pairs_of_b<kTriads>(A, a, sa, ao, ad, bi, T, wc, cat_a, exact_masks, flags, q, qn);
       __syncwarp();
     }
@@ -695,7 +697,9 @@ __global__ void k_closed_work(const uint64_t* poff, const uint32_t* plen, const 
 }  // namespace
 
 constexpr size_t closed_smem_bytes(unsigned slots) { return (sizeof(uint64_t) + sizeof(uint32_t)) * slots; }
-constexpr unsigned kBigSlots = 8192, kSmallSlots = 4096;
+// Rows longer than small_row: one 1024-thread block per SM with a
+// 16384-slot table (rows up to 8192 entries in shared memory).
+constexpr unsigned kBigSlots = 16384, kSmallSlots = 4096, kBigThreads = 1024;
 
 // Centres that own at least one oriented wedge, heaviest first.
 static int closed_worklist(hm_graph* g) {
@@ -751,11 +755,11 @@ static int closed_worklist(hm_graph* g) {
 static int prepare_static_attrs() {
   static bool attr_set = false;
   if (!attr_set) {
-    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 1, false, kBigThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)closed_smem_bytes(kBigSlots)));
     HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)closed_smem_bytes(kSmallSlots)));
-    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HM_CUDA(cudaFuncSetAttribute(k_closed<kBigSlots, 1, true, kBigThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)closed_smem_bytes(kBigSlots)));
     HM_CUDA(cudaFuncSetAttribute(k_closed<kSmallSlots, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)closed_smem_bytes(kSmallSlots)));
@@ -810,7 +814,8 @@ int prepare_static(hm_graph* g) {
 }
 
 // The closed phase over a work list split at bounds[0..3]: rows longer than
-// small_row (8192-slot tables, 2 blocks per SM), rows longer than warp_row
+// small_row (16384-slot tables, one 1024-thread block per SM; 8192-slot
+// tables at 2 blocks of 256 took 9 % longer per count at config 2), rows longer than warp_row
 // (4096-slot tables, 4 blocks per SM), then the short rows, one warp each.
 // queues holds three zeroed counters, one per launch.
 template <bool kTriads = false>
@@ -825,8 +830,8 @@ static int launch_closed(hm_ctx* ctx, ClosedArgs base, const uint32_t bounds[4],
     A.queue = queues + part;
     const uint32_t items = (n - base.shard + base.n_shards - 1) / base.n_shards;
     if (part == 0) {
-      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 2, items);
-      k_closed<kBigSlots, 2, kTriads><<<grid, kClosedBlock, closed_smem_bytes(kBigSlots), st>>>(A);
+      const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms, items);
+      k_closed<kBigSlots, 1, kTriads, kBigThreads><<<grid, kBigThreads, closed_smem_bytes(kBigSlots), st>>>(A);
     } else if (part == 1) {
       const unsigned grid = std::min<unsigned>((unsigned)ctx->n_sms * 4, items);
       k_closed<kSmallSlots, 4, kTriads><<<grid, kClosedBlock, closed_smem_bytes(kSmallSlots), st>>>(A);
@@ -1193,7 +1198,7 @@ struct EventPair {
 // moves rows between one warp and one block per centre, the small-table
 // limit moves rows between 4-per-SM and 2-per-SM blocks.
 // Only the warp limit is tuned. Moving rows of 513-2048 entries to the
-// 8192-slot shape looked 8 % faster on the strided sample of the 2M-hyperedge
+// large-row shape (then 8192 slots) looked 8 % faster on the strided sample of the 2M-hyperedge
 // config-2 graph and was 33 % slower on the whole graph (22.5 s against
 // 16.9 s per count): the sample's blocks share little of N+ in L2, the whole
 // graph's do.
